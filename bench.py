@@ -1,0 +1,280 @@
+"""Benchmark of the slime-chunk cluster search on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Workload: the full-world threshold-60 scan -- one seeded int64 world seed, every chunk centre of
+the world (radius 1,875,000 about (0,0): 3,750,001^2 = 1.40625e13 centres), the 221-cell AFK
+window, top-1,000 ranking. One step = one complete search through the C ABI
+(search_slime_clusters_gpu_v1_centered). Prints one JSON line on rank 0.
+
+  value   T centres/s from the scan kernels' own CUDA-event time (inputs on the device)
+  e2e     T centres/s of the whole C-ABI call with a host result buffer, event-timed per step
+  roofline  integer issue: 4 INT32 lane-ops per centre against the measured INT32 lane-op peak
+  cpu_baseline  the reference CPU library on a bounded square sub-area (rank 0, N=1)
+
+With N > 1 every rank runs its own replica (a different world seed) with no collective; value is
+the total centres of all ranks over the slowest rank's time (weak scaling).
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+from slime_b200 import workloads  # noqa: E402
+
+ALGO_OPS_PER_CENTRE = 4  # first-draw test per centre: add, xor, multiply-add, compare
+
+
+def env_rank():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)),
+            int(os.environ.get("WORLD_SIZE", 1)))
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, index: int):
+        self.index = index
+        self.samples = []
+        self.proc = None
+        self.thread = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.index}", f"--query-gpu={self.FIELDS}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except (OSError, FileNotFoundError):
+            self.proc = None
+            return
+        self.thread = threading.Thread(target=self._read, daemon=True)
+        self.thread.start()
+
+    def _read(self):
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) >= 9:
+                self.samples.append(parts)
+
+    def stop(self):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+        if self.thread:
+            self.thread.join(timeout=5)
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unsampled"]}
+        sm = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        mx = [float(s[2]) for s in self.samples if s[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4) if s[5 + i] == "Active"})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.samples)}
+
+
+def int_peak(core):
+    """Measured INT32 lane-op peak: the best of the integer probes (LOP3, IADD3, IMAD, mix)."""
+    rates = {}
+    for kind, name in ((0, "lop3"), (1, "iadd3"), (2, "imad"), (4, "gen_mix"), (3, "popc"),
+                       (6, "shf")):
+        core.microbench(kind, 256)  # warm
+        rates[name], _ = core.microbench(kind, 4096)
+    peak = max(rates[k] for k in ("lop3", "iadd3", "imad", "gen_mix"))
+    return peak, rates
+
+
+def flush_l2(torch, buf):
+    buf.zero_()  # writes 256 MB > 126 MB L2
+
+
+def cpu_baseline(seed: int, budget_s: float = 12.0):
+    """Reference CPU library (SlimeCore.cpp, AVX2 + OpenMP, all host threads) on a centred
+    square sub-area of the same workload, sized to about `budget_s` seconds."""
+    from oracle.oracle import REF_SO, RefCpu, Oracle
+    threads = os.cpu_count() or 1
+    if REF_SO.exists():
+        ref, kind = RefCpu(), "reference"
+    else:
+        ref, kind = Oracle(), "port"
+    radius = 2000
+    while True:
+        t0 = time.perf_counter()
+        ref.search(seed, radius, 60, 221, 0, 0, 0, 1000, threads=threads) if kind == "reference" \
+            else ref.search(seed, radius, 60, 221, 0, 0, 0, 1000, threads=threads)
+        dt = time.perf_counter() - t0
+        centres = (2 * radius + 1) ** 2
+        if dt >= budget_s / 4 or radius >= workloads.WORLD_RADIUS:
+            break
+        radius = int(min(workloads.WORLD_RADIUS, radius * min(8.0, max(1.5, ((budget_s / max(dt, 1e-3)) ** 0.5)))))
+    return {"value": centres / dt / 1e12, "unit": "T centres/s", "cores": threads, "kind": kind,
+            "sample": f"threshold-60 search of radius {radius} about (0,0) "
+                      f"({centres:.3e} centres) in {dt:.2f} s"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return
+    spec = workloads.full_world_scan()
+    vals = []
+    info = None
+    for i in range(args.warmup + args.steps):
+        info = cpu_baseline(spec.seed, budget_s=6.0 if i >= args.warmup else 2.0)
+        if i >= args.warmup:
+            vals.append(info["value"])
+    v = statistics.median(vals)
+    line = {"impl": "reference", "metric": "T centres/s full-world thr60 (plain)", "value": v,
+            "unit": "T centres/s", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "int64", "data": "synthetic",
+            "config": {"workload": "full-world threshold-60 scan (radius 1,875,000, top 1,000); "
+                                   "reference arm times bounded centred squares of it on the CPU"},
+            "cpu_baseline": {k: info[k] for k in ("value", "unit", "cores", "kind", "sample")},
+            "e2e": {"value": v, "unit": "T centres/s", "h2d_bytes_per_step": 0,
+                    "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--radius", type=int, default=workloads.WORLD_RADIUS,
+                    help="search radius in chunks (default: the full world)")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    rank, local_rank, world = env_rank()
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+
+    import numpy as np
+    import torch
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
+
+    from slime_b200 import build
+    from slime_b200.lib import RESULT_DTYPE, SlimeCoreB200
+    build.build()
+    core = SlimeCoreB200()
+    spec = workloads.full_world_scan()
+    seed = spec.seed + rank * 0x9E3779B97F4A7C15 % (1 << 63)
+    seed = ((seed + (1 << 63)) % (1 << 64)) - (1 << 63)
+    radius = min(args.radius, workloads.WORLD_RADIUS)
+    centres = (2 * radius + 1) ** 2
+    out = np.zeros(spec.max_results, dtype=RESULT_DTYPE)
+
+    peak, rates = int_peak(core)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device="cuda")
+    stream = torch.cuda.current_stream()
+
+    def step():
+        core.lib.reset_cancel()
+        return core.search(seed, radius, spec.min_size, spec.max_size, 0, 0, 0, spec.max_results,
+                           0, out=out)
+
+    for _ in range(args.warmup):
+        flush_l2(torch, flush)
+        step()
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler = ClockSampler(local_rank)
+    sampler.start()
+    kernel_ms = 0.0
+    launches = 0
+    e2e_ms = 0.0
+    totals = []
+    for _ in range(args.steps):
+        flush_l2(torch, flush)
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        total, res = step()
+        b.record(stream)
+        b.synchronize()
+        e2e_ms += a.elapsed_time(b)
+        kms, n = core.last_search_stats()
+        kernel_ms += kms
+        launches += n
+        totals.append(total)
+    torch.cuda.synchronize()
+    sampler.stop()
+    if dist:
+        dist.barrier()
+        t = torch.tensor([kernel_ms, e2e_ms], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        kernel_ms, e2e_ms = t.tolist()
+    if rank != 0:
+        if dist:
+            dist.destroy_process_group()
+        return
+
+    value = centres * args.steps * world / (kernel_ms * 1e-3) / 1e12
+    e2e = centres * args.steps * world / (e2e_ms * 1e-3) / 1e12
+    achieved_ops = value * 1e12 / world * ALGO_OPS_PER_CENTRE
+    line = {
+        "metric": "T centres/s full-world thr60 (plain)",
+        "value": value,
+        "unit": "T centres/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": kernel_ms / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "int64",
+        "data": "synthetic",
+        "config": {"workload": f"full-world threshold-60 scan, radius {radius} about (0,0) "
+                               f"({centres:.5e} centres), top {spec.max_results}",
+                   "seed": seed, "engine": core.lib.get_gpu_v1_algorithm(),
+                   "l2": "flushed between steps (256 MB write)",
+                   "parallelism": f"{world} independent replicas" if world > 1 else "1 GPU",
+                   "sites_found": totals[-1]},
+        "e2e": {"value": e2e, "unit": "T centres/s", "h2d_bytes_per_step": 40,
+                "d2h_bytes_per_step": int(min(totals[-1], spec.max_results)) * 24 + 8 + 888},
+        "gpu_launches": launches,
+        "roofline": {"bound": "int32", "achieved": achieved_ops / 1e12,
+                     "peak": peak / 1e12, "unit": "T int32 lane-ops/s",
+                     "frac": achieved_ops / peak, "traffic": None,
+                     "ops_per_centre": ALGO_OPS_PER_CENTRE,
+                     "peak_source": "measured in-process (slime_b200_microbench): best of "
+                                    "LOP3/IADD3/IMAD/generator-mix probes",
+                     "probes_T_lane_ops": {k: v / 1e12 for k, v in rates.items()}},
+        "clocks": sampler.summary(),
+    }
+    if world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(spec.seed)
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

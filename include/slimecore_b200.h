@@ -1,0 +1,135 @@
+/*
+ * slimecore_b200.h -- C ABI of libslime_b200.so, the B200 (sm_100a) slime-chunk cluster search.
+ *
+ * The first group of entry points has exactly the signatures, argument meaning, return values
+ * and error behaviour of the reference GPU library `slimecore_gpu` (SlimeCoreGPU.cu, whose
+ * extern "C" block spans lines 3034-3991) and of `score_candidates_precise` in the reference
+ * CPU library (SlimeCore.cpp:654-726), so a frontend that binds those libraries with ctypes can
+ * load this one instead. Every declaration cites the reference function it replaces.
+ *
+ * Conventions (as in the reference):
+ *  - Coordinates passed in are chunk coordinates; results carry block coordinates 16*c + 8.
+ *  - Calls are synchronous. The library serialises concurrent calls with an internal lock.
+ *  - The search returns the number of centres with min_size <= count <= max_size (not the
+ *    number written) and writes the first min(total, max_results) results ranked by
+ *    (size desc, center_x asc, center_z asc); -1 on invalid arguments or a CUDA failure.
+ *  - There is no CPU fallback: without a usable CUDA device every search returns -1.
+ */
+#ifndef SLIMECORE_B200_H
+#define SLIMECORE_B200_H
+
+#include <stdbool.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* 24-byte record, identical layout to ExtChunkResult (SlimeCoreGPU.cu:198-205). */
+typedef struct ExtChunkResult {
+    int32_t size;      /* slime chunks inside the 221-cell AFK window */
+    int32_t center_x;  /* block x of the centre chunk: 16 * cx + 8 */
+    int32_t center_z;  /* block z of the centre chunk: 16 * cz + 8 */
+    int32_t obs_count; /* precise AFK score (| (y + 1024) << 20 with Y scan), else 0 */
+    int32_t afk_x;     /* best AFK block x (centre when not scored) */
+    int32_t afk_z;     /* best AFK block z */
+} ExtChunkResult;
+
+/* ---- search (replaces SlimeCoreGPU.cu:3927-3955) ------------------------------------------- */
+
+/* search_slime_clusters_gpu_v1 (SlimeCoreGPU.cu:3927-3934): search centred on chunk (0, 0). */
+int64_t search_slime_clusters_gpu_v1(int64_t seed, int64_t rd_max, int32_t min_size,
+                                     int32_t max_size, int64_t rd_min,
+                                     ExtChunkResult* results_buffer, int32_t max_results,
+                                     int32_t precise_afk);
+
+/* search_slime_clusters_gpu_v1_centered (SlimeCoreGPU.cu:3936-3944). Centres are the
+ * (2*rd_max+1)^2 chunks around the search centre minus those with dx^2 + dz^2 < rd_min^2.
+ * With precise_afk != 0 the best min(n, 100) results are scored (SlimeCoreGPU.cu:3882-3909). */
+int64_t search_slime_clusters_gpu_v1_centered(int64_t seed, int64_t rd_max, int32_t min_size,
+                                              int32_t max_size, int64_t rd_min,
+                                              int32_t search_center_x, int32_t search_center_z,
+                                              ExtChunkResult* results_buffer, int32_t max_results,
+                                              int32_t precise_afk);
+
+/* Legacy aliases (SlimeCoreGPU.cu:3946-3965). */
+int64_t search_slime_clusters_gpu_v34(int64_t seed, int64_t rd_max, int32_t min_size,
+                                      int32_t max_size, int64_t rd_min,
+                                      ExtChunkResult* results_buffer, int32_t max_results,
+                                      int32_t precise_afk);
+int64_t search_slime_clusters_gpu_v34_centered(int64_t seed, int64_t rd_max, int32_t min_size,
+                                               int32_t max_size, int64_t rd_min,
+                                               int32_t search_center_x, int32_t search_center_z,
+                                               ExtChunkResult* results_buffer,
+                                               int32_t max_results, int32_t precise_afk);
+
+/* ---- precise AFK scoring -------------------------------------------------------------------- */
+
+/* refine_candidates_y (SlimeCoreGPU.cu:3958-3990): XZ offsets and every configured Y level;
+ * obs_count always packs Y. Semantics of the reference CPU routine (SlimeCore.cpp:728-773). */
+void refine_candidates_y(int64_t seed, ExtChunkResult* results_buffer, int32_t count);
+
+/* score_candidates_precise (SlimeCore.cpp:654-726): `threads` is accepted for signature
+ * compatibility and ignored (the work runs on the GPU). */
+void score_candidates_precise(int64_t seed, ExtChunkResult* results_buffer, int32_t count,
+                              int32_t threads, int32_t scan_xz);
+
+/* set_y_scan_config (SlimeCoreGPU.cu:3123-3140): y_step <= 0 means 4. */
+void set_y_scan_config(int32_t enabled, int32_t platform_y, int32_t y_min, int32_t y_max,
+                       int32_t y_step);
+
+/* ---- control and progress (SlimeCoreGPU.cu:3085-3116) --------------------------------------- */
+
+void request_cancel(void);
+void request_pause(void);
+void resume_search(void);
+void reset_cancel(void);
+int32_t get_progress(void);
+int64_t get_processed_centers(void);
+int64_t get_gpu_scan_work_ns(void);
+
+/* ---- device and diagnostics (SlimeCoreGPU.cu:3035-3083,3118-3161) --------------------------- */
+
+int32_t get_cuda_device_count(void);
+int32_t get_cuda_device_name(char* buffer, int32_t buffer_size);
+int32_t get_gpu_v1_shape(void);
+int32_t get_gpu_v1_algorithm(void);
+int32_t get_gpu_v1_rng(void);
+void set_gpu_v1_rng_override(int32_t value);
+int32_t get_gpu_v34_shape(void);
+int32_t get_gpu_v34_rng(void);
+void set_gpu_v34_rng_override(int32_t value);
+/* Releases this library's device buffers and stream. Unlike the reference
+ * (SlimeCoreGPU.cu:3118-3121) it never resets the device. */
+void cleanup_gpu_resources(void);
+/* is_slime_chunk_c (SlimeCoreGPU.cu:3142-3161). */
+bool is_slime_chunk_c(int64_t seed, int64_t cx, int64_t cz);
+
+/* ---- additions of this library (no reference counterpart) ----------------------------------- */
+
+/* Library version string. */
+const char* slime_b200_version(void);
+
+/* Statistics of the last search call: summed duration of its scan kernels, timed with CUDA events
+ * on the library's stream, and the number of kernels it launched. */
+void slime_b200_last_search_stats(double* kernel_ms, int64_t* launches);
+
+/* Last CUDA error text of this library ("" if none). */
+const char* slime_b200_last_error(void);
+
+/* out[i] = is_slime(seed, x[i], z[i]) for n host-resident coordinates, evaluated on the GPU.
+ * Returns 0, or -1 on a CUDA failure. */
+int32_t slime_b200_is_slime_batch(int64_t seed, const int64_t* x, const int64_t* z, uint8_t* out,
+                                  int64_t n);
+
+/* Integer-pipe throughput probe on the current device (the denominator of the scan's roofline).
+ * kind: 0 LOP3, 1 IADD3, 2 IMAD, 3 POPC, 4 generator mix (IADD3+LOP3+IMAD+ISETP+VOTE),
+ * 5 b1 tensor AND+POPC (mma.sync m16n8k256), 6 SHF. Writes lane operations per second and the
+ * timed milliseconds. Returns 0, or -1 on a CUDA failure. */
+int32_t slime_b200_microbench(int32_t kind, int32_t iters, double* lane_ops_per_s, double* ms);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* SLIMECORE_B200_H */

@@ -1,0 +1,113 @@
+// driver.h -- process-wide state of the C-ABI library (one device, one stream, cached buffers).
+#pragma once
+
+#include <atomic>
+#include <cstdint>
+#include <mutex>
+#include <string>
+#include <vector>
+
+#include <cuda_runtime.h>
+
+#include "slime_core.cuh"
+
+namespace slime {
+
+// Device buffer that only grows; freed by cleanup_gpu_resources().
+template <typename T>
+struct DeviceBuffer {
+    T* ptr = nullptr;
+    size_t count = 0;
+    cudaError_t reserve(size_t n) {
+        if (n <= count) return cudaSuccess;
+        free();
+        const cudaError_t e = cudaMalloc(&ptr, n * sizeof(T));
+        if (e != cudaSuccess) {
+            ptr = nullptr;
+            return e;
+        }
+        count = n;
+        return cudaSuccess;
+    }
+    void free() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        count = 0;
+    }
+};
+
+struct SearchSpec {
+    int64_t seed;
+    int64_t rd_max;
+    int32_t min_size;
+    int32_t max_size;
+    int64_t rd_min;
+    int32_t center_x;
+    int32_t center_z;
+    int32_t max_results;
+    int32_t precise_afk;
+};
+
+// Values reported by get_gpu_v1_algorithm().
+constexpr int32_t kAlgoGeneral = 100;
+constexpr int32_t kAlgoBand = 200;
+
+constexpr size_t kPinnedBytes = 1 << 20;
+
+// Result entries the scan may materialise per launch: at least 4M, and 4x the requested top-K.
+inline size_t hit_capacity(int32_t max_results) {
+    const size_t k = (size_t)(max_results > 0 ? max_results : 1) * 4;
+    return k > (4u << 20) ? k : (4u << 20);
+}
+
+bool validate_search(int64_t rd_max, int32_t min_size, int32_t max_size, int64_t rd_min,
+                     int32_t cx, int32_t cz, const void* results, int32_t max_results);
+
+struct Context {
+    std::mutex mu;
+    int device = -1;
+    int sm_count = 148;
+    cudaStream_t stream = nullptr;
+    void* pinned = nullptr;
+    std::string last_error;
+
+    DeviceBuffer<uint64_t> xt, zt;
+    DeviceBuffer<Hit> hits;
+    DeviceBuffer<unsigned long long> counters;
+    DeviceBuffer<unsigned int> hist;
+    DeviceBuffer<ExtChunkResult> sites;
+
+    // Y-scan configuration (set_y_scan_config) and the tables built from it.
+    int32_t y_enabled = 0, platform_y = -64, y_min = -64, y_max = 64, y_step = 4;
+    bool y_ready = false;
+    int32_t y_count = 1;
+    DeviceBuffer<int32_t> y_values;
+    DeviceBuffer<int16_t> outer, inner;
+    DeviceBuffer<uint16_t> weights;
+
+    // Control plane (polled between slabs).
+    std::atomic<int> cancel{0}, paused{0}, progress{0};
+    std::atomic<int64_t> processed{0}, work_ns{0};
+    int32_t last_algorithm = -1, last_shape = 0, rng_override = -1;
+
+    // Statistics of the last search: kernel time measured with CUDA events on the library's
+    // stream around every scan launch, and the number of kernels this library launched.
+    double last_kernel_ms = 0.0;
+    int64_t last_launches = 0;
+    cudaEvent_t ev_a = nullptr, ev_b = nullptr;
+
+    void set_error(const char* where, cudaError_t e);
+    bool ensure_device();
+    bool ensure_y_tables();
+    void release();
+    void release_extra();
+
+    bool scan_general(const SearchSpec& q, std::vector<Hit>& best, std::vector<uint32_t>& hist_out,
+                      bool& cancelled);
+    bool score(int64_t seed, ExtChunkResult* host, int32_t n, int32_t scan_xz, bool pack);
+    int64_t search(const SearchSpec& q, ExtChunkResult* results);
+};
+
+Context& ctx();
+
+}  // namespace slime

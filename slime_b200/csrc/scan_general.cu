@@ -1,0 +1,188 @@
+// scan_general.cu -- the general-purpose scan: any area, any threshold, exact predicate.
+//
+// Behaviour follows the reference GPU search (SlimeCoreGPU.cu:501-610, 3164-3851): every centre
+// of the area whose exact 221-cell count lies in [min_size, max_size] (outside the rd_min disc)
+// is kept. Design on B200: a persistent grid walks (x tile, z band) tiles; each warp evaluates
+// 32 x-adjacent chunks per ballot and publishes the words of a row into a 32-row shared ring;
+// each thread keeps rolling 17x17 square counts for its centre columns (square >= circle and
+// square - 68 <= circle), and only square survivors get the exact circle count. Kept centres are
+// histogrammed by count and those at or above `emit_min` are appended with one atomic per warp.
+#include "engine.h"
+
+namespace slime {
+namespace {
+
+constexpr unsigned kFull = 0xFFFFFFFFu;
+
+template <int TPB, int CPT>
+struct GeneralTile {
+    static constexpr int kWarps = TPB / 32;
+    static constexpr int kWords = kWarps * CPT;   // 32-bit words per ring row
+    static constexpr int kStride = kWords + 4;    // + zero padding word(s), 16-byte rows
+    static constexpr int kInW = kWords * 32;
+    static constexpr int kOutW = kInW - 16;
+};
+
+__device__ __forceinline__ uint32_t slice17(const uint32_t* row, int word, int lane) {
+    return __funnelshift_r(row[word], row[word + 1], lane) & 0x1FFFFu;
+}
+
+template <int TPB, int CPT>
+__global__ void __launch_bounds__(TPB) general_scan_kernel(const ScanArgs a) {
+    using T = GeneralTile<TPB, CPT>;
+    __shared__ __align__(16) uint32_t ring[32 * T::kStride];
+    __shared__ unsigned int hist_s[kHistBins];
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    for (int i = tid; i < kHistBins; i += TPB) hist_s[i] = 0;
+    for (int i = tid; i < 32 * (T::kStride - T::kWords); i += TPB)
+        ring[(i / (T::kStride - T::kWords)) * T::kStride + T::kWords +
+             i % (T::kStride - T::kWords)] = 0;
+    __syncthreads();
+
+    const int64_t tiles = (int64_t)a.tiles_x * a.tiles_z;
+    const bool no_upper = a.max_size >= 221;
+    for (int64_t t = blockIdx.x; t < tiles; t += gridDim.x) {
+        const int x_base = (int)(t % a.tiles_x) * T::kOutW;
+        const int z_base = a.slab_z0 + (int)(t / a.tiles_x) * a.band_h;
+        const int out_w = min(T::kOutW, a.width - x_base);
+        const int out_h = min(a.band_h, a.slab_z0 + a.slab_h - z_base);
+        const int in_w = out_w + 16, in_h = out_h + 16;
+
+        uint64_t xt[CPT];
+        int sq[CPT];
+#pragma unroll
+        for (int k = 0; k < CPT; ++k) {
+            const int col = (warp * CPT + k) * 32 + lane;
+            xt[k] = col < in_w ? a.xt[x_base + col] : 0;
+            sq[k] = 0;
+        }
+
+        for (int r = 0; r < in_h; ++r) {
+            const uint64_t zt = a.zt[z_base + r];
+            uint32_t words[CPT];
+#pragma unroll
+            for (int k = 0; k < CPT; ++k) {
+                const int col = (warp * CPT + k) * 32 + lane;
+                words[k] = __ballot_sync(kFull, col < in_w && slime_from_terms(xt[k], zt));
+            }
+            uint32_t* row = ring + (r & 31) * T::kStride;
+            if (lane == 0) {
+#pragma unroll
+                for (int k = 0; k < CPT; k += (CPT >= 4 ? 4 : 1)) {
+                    if constexpr (CPT >= 4)
+                        *reinterpret_cast<uint4*>(row + warp * CPT + k) =
+                            make_uint4(words[k], words[k + 1], words[k + 2], words[k + 3]);
+                    else
+                        row[warp * CPT + k] = words[k];
+                }
+            }
+            __syncthreads();
+
+#pragma unroll
+            for (int k = 0; k < CPT; ++k) {
+                const int word = warp * CPT + k;
+                const int col = word * 32 + lane;
+                const bool active = col < out_w;
+                if (active) {
+                    sq[k] += __popc(slice17(row, word, lane));
+                    if (r >= 17) sq[k] -= __popc(slice17(ring + ((r - 17) & 31) * T::kStride, word, lane));
+                }
+                bool want = false;
+                int exact = 0;
+                int cz = 0;
+                if (active && r >= 16 && sq[k] >= a.min_size && (no_upper || sq[k] <= a.max_size + 68)) {
+                    const int j = r - 16;  // centre row within the tile
+                    const int cx = a.area_x0 + x_base + col;
+                    cz = a.area_z0 + z_base + j;
+                    bool inside = true;
+                    if (a.rd_min_sq != 0) {
+                        const int64_t dx = (int64_t)cx - a.center_x, dz = (int64_t)cz - a.center_z;
+                        inside = dx * dx + dz * dz >= a.rd_min_sq;
+                    }
+                    if (inside) {
+#pragma unroll
+                        for (int i = 0; i < 17; ++i)
+                            exact += __popc(slice17(ring + ((j + i) & 31) * T::kStride, word, lane) &
+                                            window_row_mask(i));
+                        if (exact >= a.min_size && exact <= a.max_size) {
+                            atomicAdd(&hist_s[exact], 1u);
+                            want = exact >= a.emit_min;
+                        }
+                    }
+                }
+                const unsigned m = __ballot_sync(kFull, want);
+                if (m) {
+                    const int leader = __ffs(m) - 1;
+                    unsigned long long base = 0;
+                    if (lane == leader) base = atomicAdd(a.emitted, (unsigned long long)__popc(m));
+                    base = __shfl_sync(kFull, base, leader);
+                    if (want) {
+                        const unsigned long long idx = base + __popc(m & ((1u << lane) - 1u));
+                        if (idx < a.cap) a.out[idx] = Hit{exact, a.area_x0 + x_base + col, cz};
+                    }
+                }
+            }
+        }
+        __syncthreads();  // the next tile reuses ring slots still read above
+    }
+    for (int i = tid; i < kHistBins; i += TPB)
+        if (hist_s[i]) atomicAdd(&a.hist[i], hist_s[i]);
+}
+
+__global__ void terms_kernel(uint64_t* xt, int32_t x0, int32_t nx, uint64_t* zt, int32_t z0,
+                             int32_t nz, int64_t seed) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nx) xt[i] = x_term((int32_t)((int64_t)x0 + i));
+    if (i < nz) zt[i] = z_term((int32_t)((int64_t)z0 + i)) + (uint64_t)seed;
+}
+
+__global__ void predicate_kernel(int64_t seed, const int64_t* x, const int64_t* z, uint8_t* out,
+                                 int64_t n) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = is_slime(seed, x[i], z[i]) ? 1 : 0;
+}
+
+constexpr int kWideTpb = 256, kWideCpt = 4;
+constexpr int kNarrowTpb = 256, kNarrowCpt = 1;
+
+}  // namespace
+
+int general_out_width(bool narrow) {
+    return narrow ? GeneralTile<kNarrowTpb, kNarrowCpt>::kOutW : GeneralTile<kWideTpb, kWideCpt>::kOutW;
+}
+
+int general_max_grid(bool narrow) {
+    int dev = 0, sms = 0, per_sm = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (narrow)
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, general_scan_kernel<kNarrowTpb, kNarrowCpt>, kNarrowTpb, 0);
+    else
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, general_scan_kernel<kWideTpb, kWideCpt>, kWideTpb, 0);
+    return (sms > 0 ? sms : 148) * (per_sm > 0 ? per_sm : 1);
+}
+
+cudaError_t launch_general_scan(const ScanArgs& a, bool narrow, int grid, cudaStream_t s) {
+    if (narrow)
+        general_scan_kernel<kNarrowTpb, kNarrowCpt><<<grid, kNarrowTpb, 0, s>>>(a);
+    else
+        general_scan_kernel<kWideTpb, kWideCpt><<<grid, kWideTpb, 0, s>>>(a);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_terms(uint64_t* xt, int32_t x0, int32_t nx, uint64_t* zt, int32_t z0,
+                         int32_t nz, int64_t seed, cudaStream_t s) {
+    const int32_t n = nx > nz ? nx : nz;
+    terms_kernel<<<(n + 255) / 256, 256, 0, s>>>(xt, x0, nx, zt, z0, nz, seed);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_predicate(int64_t seed, const int64_t* x, const int64_t* z, uint8_t* out,
+                             int64_t n, cudaStream_t s) {
+    if (n <= 0) return cudaSuccess;
+    predicate_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(seed, x, z, out, n);
+    return cudaGetLastError();
+}
+
+}  // namespace slime

@@ -1,0 +1,129 @@
+"""ctypes binding of libslime_b200.so -- the same entry points a ctypes frontend of the reference
+GPU library (`slimecore_gpu`) binds, plus this library's additions.
+
+There is no fallback: if the shared library is missing or no CUDA device is usable, calls fail
+loudly (the search returns -1 and :class:`SlimeCoreB200` raises).
+"""
+from __future__ import annotations
+
+import ctypes as C
+from pathlib import Path
+
+import numpy as np
+
+from .build import LIB
+
+RESULT_DTYPE = np.dtype(
+    [("size", "<i4"), ("center_x", "<i4"), ("center_z", "<i4"), ("obs_count", "<i4"),
+     ("afk_x", "<i4"), ("afk_z", "<i4")]
+)
+
+i64, i32, vp, u8p = C.c_int64, C.c_int32, C.c_void_p, C.c_void_p
+
+# name -> (restype, argtypes); one line per symbol of include/slimecore_b200.h.
+SIGNATURES = {
+    "search_slime_clusters_gpu_v1": (i64, [i64, i64, i32, i32, i64, vp, i32, i32]),
+    "search_slime_clusters_gpu_v1_centered": (i64, [i64, i64, i32, i32, i64, i32, i32, vp, i32, i32]),
+    "search_slime_clusters_gpu_v34": (i64, [i64, i64, i32, i32, i64, vp, i32, i32]),
+    "search_slime_clusters_gpu_v34_centered": (i64, [i64, i64, i32, i32, i64, i32, i32, vp, i32, i32]),
+    "refine_candidates_y": (None, [i64, vp, i32]),
+    "score_candidates_precise": (None, [i64, vp, i32, i32, i32]),
+    "set_y_scan_config": (None, [i32, i32, i32, i32, i32]),
+    "request_cancel": (None, []),
+    "request_pause": (None, []),
+    "resume_search": (None, []),
+    "reset_cancel": (None, []),
+    "get_progress": (i32, []),
+    "get_processed_centers": (i64, []),
+    "get_gpu_scan_work_ns": (i64, []),
+    "get_cuda_device_count": (i32, []),
+    "get_cuda_device_name": (i32, [C.c_char_p, i32]),
+    "get_gpu_v1_shape": (i32, []),
+    "get_gpu_v1_algorithm": (i32, []),
+    "get_gpu_v1_rng": (i32, []),
+    "set_gpu_v1_rng_override": (None, [i32]),
+    "get_gpu_v34_shape": (i32, []),
+    "get_gpu_v34_rng": (i32, []),
+    "set_gpu_v34_rng_override": (None, [i32]),
+    "cleanup_gpu_resources": (None, []),
+    "is_slime_chunk_c": (C.c_bool, [i64, i64, i64]),
+    "slime_b200_version": (C.c_char_p, []),
+    "slime_b200_last_error": (C.c_char_p, []),
+    "slime_b200_last_search_stats": (None, [C.POINTER(C.c_double), C.POINTER(i64)]),
+    "slime_b200_is_slime_batch": (i32, [i64, vp, vp, u8p, i64]),
+    "slime_b200_microbench": (i32, [i32, i32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
+}
+
+
+def load(path: Path | str = LIB) -> C.CDLL:
+    path = Path(path)
+    if not path.exists():
+        raise FileNotFoundError(f"{path} is not built; run `python -m slime_b200.build`")
+    lib = C.CDLL(str(path))
+    for name, (res, args) in SIGNATURES.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    return lib
+
+
+def _ptr(a: np.ndarray):
+    return a.ctypes.data_as(C.c_void_p)
+
+
+class SlimeError(RuntimeError):
+    pass
+
+
+class SlimeCoreB200:
+    """Pythonic view of the C ABI; every call goes through the exported C functions."""
+
+    def __init__(self, path: Path | str = LIB):
+        self.lib = load(path)
+
+    def _check(self, ok: bool, what: str):
+        if not ok:
+            raise SlimeError(f"{what} failed: {self.lib.slime_b200_last_error().decode()}")
+
+    def search(self, seed: int, rd_max: int, min_size: int, max_size: int = 221, rd_min: int = 0,
+               center_x: int = 0, center_z: int = 0, max_results: int = 1000,
+               precise_afk: int = 0, out: np.ndarray | None = None):
+        """search_slime_clusters_gpu_v1_centered; returns (total, ranked results)."""
+        buf = out if out is not None else np.zeros(max(max_results, 1), dtype=RESULT_DTYPE)
+        total = self.lib.search_slime_clusters_gpu_v1_centered(
+            seed, rd_max, min_size, max_size, rd_min, center_x, center_z, _ptr(buf), max_results,
+            precise_afk)
+        self._check(total >= 0, "search")
+        return total, buf[: min(total, max_results)]
+
+    def score_precise(self, seed: int, sites: np.ndarray, scan_xz: int = 1) -> np.ndarray:
+        buf = np.ascontiguousarray(sites, dtype=RESULT_DTYPE).copy()
+        self.lib.score_candidates_precise(seed, _ptr(buf), len(buf), 0, scan_xz)
+        return buf
+
+    def refine_y(self, seed: int, sites: np.ndarray) -> np.ndarray:
+        buf = np.ascontiguousarray(sites, dtype=RESULT_DTYPE).copy()
+        self.lib.refine_candidates_y(seed, _ptr(buf), len(buf))
+        return buf
+
+    def set_y_scan_config(self, enabled=0, platform_y=-64, y_min=-64, y_max=64, y_step=4):
+        self.lib.set_y_scan_config(enabled, platform_y, y_min, y_max, y_step)
+
+    def is_slime_batch(self, seed: int, x: np.ndarray, z: np.ndarray) -> np.ndarray:
+        x = np.ascontiguousarray(x, dtype=np.int64)
+        z = np.ascontiguousarray(z, dtype=np.int64)
+        out = np.zeros(len(x), dtype=np.uint8)
+        self._check(self.lib.slime_b200_is_slime_batch(seed, _ptr(x), _ptr(z), _ptr(out), len(x)) == 0,
+                    "is_slime_batch")
+        return out
+
+    def last_search_stats(self):
+        ms, n = C.c_double(), C.c_int64()
+        self.lib.slime_b200_last_search_stats(C.byref(ms), C.byref(n))
+        return ms.value, n.value
+
+    def microbench(self, kind: int, iters: int = 4096):
+        ops, ms = C.c_double(), C.c_double()
+        self._check(self.lib.slime_b200_microbench(kind, iters, C.byref(ops), C.byref(ms)) == 0,
+                    "microbench")
+        return ops.value, ms.value
