@@ -114,6 +114,16 @@ const char* slime_b200_version(void);
  * on the library's stream, and the number of kernels it launched. */
 void slime_b200_last_search_stats(double* kernel_ms, int64_t* launches);
 
+/* Rare redraw chunks (first draw rejected by nextInt(10), redraw slime) found by the last search
+ * that used the band engine; 0 otherwise. */
+int64_t slime_b200_last_rare_chunks(void);
+
+/* Engine selection: mode 0 automatic, 1 always the general scan, 2 the band engine whenever the
+ * threshold allows it (min_size >= 28). `band_min_threshold` (28..221, other values keep the
+ * current one) is the smallest threshold automatic mode sends to the band engine. Results are
+ * identical either way; only speed differs. */
+void slime_b200_set_engine(int32_t mode, int32_t band_min_threshold);
+
 /* Last CUDA error text of this library ("" if none). */
 const char* slime_b200_last_error(void);
 

@@ -22,6 +22,7 @@ import numpy as np
 HERE = Path(__file__).resolve().parent
 ORACLE_SO = HERE / "_build" / "libslime_oracle.so"
 REF_SO = HERE / "_ref" / "libslimecore_ref.so"
+REF_GPU_SO = HERE / "_ref" / "libslimecore_gpu_ref.so"
 REF_SRC_DIR = Path(os.environ.get("SLIME_REFERENCE_DIR", "/root/reference"))
 
 
@@ -53,8 +54,8 @@ def build(ref: bool = True) -> None:
     """Build the restatement, and the reference CPU library when its source is present."""
     subprocess.run(["make", "-C", str(HERE), "oracle"], check=True, capture_output=True)
     if ref and (REF_SRC_DIR / "SlimeCore.cpp").exists():
-        subprocess.run(["make", "-C", str(HERE), "ref", f"REF_DIR={REF_SRC_DIR}"], check=True,
-                       capture_output=True)
+        subprocess.run(["make", "-C", str(HERE), "ref", "ref_gpu", f"REF_DIR={REF_SRC_DIR}"],
+                       check=True, capture_output=True)
 
 
 def _ptr(a: np.ndarray):
@@ -178,6 +179,34 @@ class RefCpu:
         buf = np.ascontiguousarray(results, dtype=RESULT_DTYPE).copy()
         self.lib.refine_candidates_y(seed, _ptr(buf), len(buf), threads or os.cpu_count())
         return buf
+
+
+class RefGpu:
+    """The reference's GPU library, compiled from SlimeCoreGPU.cu for sm_100a (a checker for
+    areas too large for the CPU). Its cleanup_gpu_resources() resets the device and is never
+    called."""
+
+    def __init__(self, path: Path = REF_GPU_SO):
+        if not Path(path).exists():
+            raise FileNotFoundError(f"{path} is not built (needs the reference source tree)")
+        lib = C.CDLL(str(path))
+        i64, i32, vp = C.c_int64, C.c_int32, C.c_void_p
+        lib.search_slime_clusters_gpu_v1_centered.argtypes = [i64, i64, i32, i32, i64, i32, i32,
+                                                              vp, i32, i32]
+        lib.search_slime_clusters_gpu_v1_centered.restype = i64
+        lib.get_processed_centers.restype = i64
+        lib.reset_cancel.argtypes = []
+        self.lib = lib
+
+    def search(self, seed, rd_max, min_size, max_size, rd_min=0, center_x=0, center_z=0,
+               max_results=1000, precise_afk=0):
+        out = empty_results(max_results)
+        self.lib.reset_cancel()
+        total = self.lib.search_slime_clusters_gpu_v1_centered(seed, rd_max, min_size, max_size,
+                                                               rd_min, center_x, center_z,
+                                                               _ptr(out), max_results, precise_afk)
+        n = 0 if total < 0 else min(total, max_results)
+        return total, out[:n].copy()
 
 
 def python_is_slime(seed: int, cx: int, cz: int) -> bool:

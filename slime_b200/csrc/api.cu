@@ -148,15 +148,7 @@ double log_tail(int s) {
     return acc;
 }
 
-// Chunk coordinates to the reference's 32-bit block coordinate (wraps like the reference).
-inline int32_t block_of(int32_t c) { return (int32_t)((uint32_t)c * 16u + 8u); }
-
-inline bool hit_better(const Hit& a, const Hit& b) {
-    if (a.count != b.count) return a.count > b.count;
-    const int32_t ax = block_of(a.cx), bx = block_of(b.cx);
-    if (ax != bx) return ax < bx;
-    return block_of(a.cz) < block_of(b.cz);
-}
+inline bool hit_better(const Hit& a, const Hit& b) { return hit_order(a, b); }
 
 void keep_best(std::vector<Hit>& v, size_t k) {
     if (v.size() > k) {
@@ -353,9 +345,11 @@ int64_t Context::search(const SearchSpec& q, ExtChunkResult* results) {
     std::vector<Hit> best;
     std::vector<uint32_t> h(kHistBins, 0u);
     bool cancelled = false;
-    last_algorithm = kAlgoGeneral;
-    last_shape = (2 * q.rd_max + 1) < 8192 ? 1 : 2;
-    if (!scan_general(q, best, h, cancelled)) {
+    last_rare = 0;
+    const bool band = band_eligible(q);
+    last_algorithm = band ? kAlgoBand : kAlgoGeneral;
+    last_shape = band ? 3 : (2 * q.rd_max + 1) < 8192 ? 1 : 2;
+    if (!(band ? scan_band(q, best, h, cancelled) : scan_general(q, best, h, cancelled))) {
         progress.store(0);
         return -1;
     }
@@ -529,6 +523,14 @@ const char* slime_b200_version(void) { return "slime_b200 0.1 (sm_100a)"; }
 void slime_b200_last_search_stats(double* kernel_ms, int64_t* launches) {
     if (kernel_ms) *kernel_ms = ctx().last_kernel_ms;
     if (launches) *launches = ctx().last_launches;
+}
+
+int64_t slime_b200_last_rare_chunks(void) { return ctx().last_rare; }
+
+void slime_b200_set_engine(int32_t mode, int32_t band_min_threshold) {
+    std::lock_guard<std::mutex> lock(ctx().mu);
+    ctx().engine_override = (mode >= 0 && mode <= 2) ? mode : 0;
+    if (band_min_threshold >= 28 && band_min_threshold <= 221) ctx().band_min_threshold = band_min_threshold;
 }
 
 const char* slime_b200_last_error(void) { return ctx().last_error.c_str(); }

@@ -1,0 +1,249 @@
+// band_driver.cu -- host side of the band engine (scan_band.cu) and its redraw correction.
+#include <algorithm>
+#include <chrono>
+#include <thread>
+#include <vector>
+
+#include "band_math.cuh"
+#include "driver.h"
+#include "engine.h"
+
+namespace slime {
+
+namespace {
+constexpr int64_t kP = band::kPeriod;
+constexpr uint32_t kRareCap = 1u << 20;
+}  // namespace
+
+bool Context::ensure_band() {
+    if (band_ready) return true;
+    cudaError_t e = band_prepare();
+    if (e != cudaSuccess) { set_error("band smem", e); return false; }
+    std::vector<uint64_t> t;
+    std::vector<uint32_t> o;
+    rare_target_table(t, o);
+    if ((e = rare_targets.reserve(t.size())) != cudaSuccess || (e = rare_offsets.reserve(o.size())) != cudaSuccess ||
+        (e = flags.reserve(4)) != cudaSuccess || (e = rare.reserve(kRareCap)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(rare_targets.ptr, t.data(), t.size() * 8, cudaMemcpyHostToDevice, stream)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(rare_offsets.ptr, o.data(), o.size() * 4, cudaMemcpyHostToDevice, stream)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(stream)) != cudaSuccess) {
+        set_error("rare table", e);
+        return false;
+    }
+    band_ready = true;
+    return true;
+}
+
+// The band engine needs a threshold >= 28 (its byte-lane bound test); automatic selection also
+// wants an area spanning two periods on one axis and a threshold high enough for its bound.
+bool Context::band_eligible(const SearchSpec& q) const {
+    if (q.min_size < 28 || engine_override == 1) return false;
+    if (engine_override == 2) return true;
+    const int64_t w = 2 * q.rd_max + 1;
+    return w >= 2 * kP && q.min_size >= band_min_threshold;
+}
+
+bool Context::scan_band(const SearchSpec& q, std::vector<Hit>& best, std::vector<uint32_t>& h,
+                        bool& cancelled) {
+    if (!ensure_band()) return false;
+    const int64_t W = 2 * q.rd_max + 1, H = W;
+    const int32_t area_x0 = (int32_t)((int64_t)q.center_x - q.rd_max);
+    const int32_t area_z0 = (int32_t)((int64_t)q.center_z - q.rd_max);
+    const bool transposed = W < 2 * kP && H >= 2 * kP;
+    const int64_t width_u = transposed ? H : W, height_v = transposed ? W : H;
+    const int64_t nI = (width_u + kP - 1) / kP, nJ = (height_v + kP - 1) / kP;
+    const int32_t ubase = (int32_t)std::min(kP, width_u), vbase = (int32_t)std::min(kP, height_v);
+    const int32_t vrows = vbase + 16;
+    const int32_t rstride = (int32_t)(1 + nJ);
+    const int out_w = band_tile_out_w();
+    cudaError_t e;
+    if ((e = xt.reserve((size_t)width_u + 16)) != cudaSuccess ||
+        (e = rt.reserve((size_t)vrows * rstride)) != cudaSuccess ||
+        (e = counters.reserve(4)) != cudaSuccess ||
+        (e = hits.reserve(hit_capacity(q.max_results))) != cudaSuccess ||
+        (e = fixed.reserve(1u << 20)) != cudaSuccess) {
+        set_error("alloc", e);
+        return false;
+    }
+    const int32_t col_first = (transposed ? area_z0 : area_x0) - 8;
+    const int32_t row_first = (transposed ? area_x0 : area_z0) - 8;
+    if ((e = launch_band_terms(xt.ptr, col_first, (int32_t)(width_u + 16), rt.ptr, rstride, vrows,
+                               (int32_t)nJ, row_first, height_v + 16, q.seed, transposed, stream)) != cudaSuccess) {
+        set_error("band terms", e);
+        return false;
+    }
+    last_launches += 2;
+
+    // Rare redraw chunks of the area and its 8-chunk halo, found before the scan so that the
+    // scan's hits can be filtered on the device.
+    if ((e = cudaMemsetAsync(flags.ptr, 0, 16, stream)) != cudaSuccess ||
+        (e = launch_rare_scan(rare_targets.ptr, rare_offsets.ptr, q.seed, area_z0 - 8, (int32_t)(H + 16),
+                              area_x0 - 8, (int32_t)(W + 16), rare.ptr, kRareCap, flags.ptr + 2, stream)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(pinned, flags.ptr + 2, 4, cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(stream)) != cudaSuccess) {
+        set_error("rare scan", e);
+        return false;
+    }
+    ++last_launches;
+    const uint32_t nrare = *(uint32_t*)pinned;
+    if (nrare > kRareCap) { set_error("too many rare chunks", cudaErrorMemoryAllocation); return false; }
+    last_rare = nrare;
+
+    const int nb_max = band_max_bands();
+    const int64_t ngroups = (nJ + nb_max - 1) / nb_max;
+    const int32_t band_h = (int32_t)std::min<int64_t>(2048, std::max<int64_t>(256, vbase));
+    const int64_t u_tiles = (ubase + out_w - 1) / out_w, v_tiles = (vbase + band_h - 1) / band_h;
+    const int64_t pairs = (nI + 1) / 2;
+    const int grid = sm_count;
+    const uint64_t cap = hits.count;
+
+    for (int64_t g = 0; g < ngroups; ++g) {
+        const int32_t per = (int32_t)((nJ + ngroups - 1) / ngroups);
+        const int32_t j0 = (int32_t)(g * per);
+        const int32_t nb = (int32_t)std::min<int64_t>(per, nJ - j0);
+        if (nb <= 0) break;
+        const int64_t tiles = u_tiles * v_tiles * pairs;
+        int64_t chunk = std::max<int64_t>(grid, std::min<int64_t>(tiles, (int64_t)grid * 24));
+        for (int64_t t0 = 0; t0 < tiles;) {
+            while (paused.load() && !cancel.load()) std::this_thread::sleep_for(std::chrono::milliseconds(20));
+            if (cancel.load()) { cancelled = true; return true; }
+            const int64_t t1 = std::min(tiles, t0 + chunk);
+            BandArgs a{};
+            a.ct = xt.ptr;
+            a.ncols = width_u + 16;
+            a.rt = rt.ptr;
+            a.rstride = rstride;
+            a.vrows = vrows;
+            a.vbase = vbase;
+            a.ubase = ubase;
+            a.width_u = width_u;
+            a.height_v = height_v;
+            a.j0 = j0;
+            a.nb = nb;
+            a.u_tiles = (int32_t)u_tiles;
+            a.v_tiles = (int32_t)v_tiles;
+            a.band_h = band_h;
+            a.tile_begin = t0;
+            a.tile_end = t1;
+            a.min_size = q.min_size;
+            a.max_size = q.max_size;
+            a.rd_min_sq = q.rd_min * q.rd_min;
+            a.area_x0 = area_x0;
+            a.area_z0 = area_z0;
+            a.center_x = q.center_x;
+            a.center_z = q.center_z;
+            a.transposed = transposed ? 1 : 0;
+            a.out = hits.ptr;
+            a.cap = cap;
+            a.emitted = counters.ptr;
+            a.overflow = flags.ptr;
+            const auto c0 = std::chrono::steady_clock::now();
+            if ((e = cudaMemsetAsync(counters.ptr, 0, 8, stream)) != cudaSuccess ||
+                (e = cudaEventRecord(ev_a, stream)) != cudaSuccess ||
+                (e = launch_band_scan(a, (int)std::min<int64_t>(grid, t1 - t0), stream)) != cudaSuccess ||
+                (e = cudaEventRecord(ev_b, stream)) != cudaSuccess ||
+                (e = cudaMemcpyAsync(pinned, counters.ptr, 8, cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
+                (e = cudaStreamSynchronize(stream)) != cudaSuccess) {
+                set_error("band scan", e);
+                return false;
+            }
+            const auto c1 = std::chrono::steady_clock::now();
+            float kms = 0.f;
+            cudaEventElapsedTime(&kms, ev_a, ev_b);
+            last_kernel_ms += kms;
+            ++last_launches;
+            const uint64_t emitted = *(unsigned long long*)pinned;
+            if (emitted > cap) {
+                if (t1 - t0 <= 1) { set_error("band hit buffer overflow", cudaErrorMemoryAllocation); return false; }
+                chunk = std::max<int64_t>(1, (t1 - t0) / 2);
+                continue;
+            }
+            work_ns.fetch_add(std::max<int64_t>(1, std::chrono::duration_cast<std::chrono::nanoseconds>(c1 - c0).count()));
+            if (emitted) {
+                if ((e = launch_filter_hits(hits.ptr, (int64_t)emitted, rare.ptr, (int32_t)nrare, stream)) != cudaSuccess) {
+                    set_error("filter", e);
+                    return false;
+                }
+                if (nrare) ++last_launches;
+                const size_t old = best.size();
+                best.resize(old + emitted);
+                if ((e = cudaMemcpyAsync(best.data() + old, hits.ptr, emitted * sizeof(Hit), cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
+                    (e = cudaStreamSynchronize(stream)) != cudaSuccess) {
+                    set_error("copy", e);
+                    return false;
+                }
+                size_t w = old;
+                for (size_t i = old; i < best.size(); ++i) {
+                    if (best[i].count < 0) continue;  // window holds a rare chunk: fixed below
+                    ++h[best[i].count];
+                    best[w++] = best[i];
+                }
+                best.resize(w);
+                if (best.size() > 2 * (size_t)q.max_results + 1000000) {
+                    std::nth_element(best.begin(), best.begin() + q.max_results, best.end(),
+                                     [](const Hit& x, const Hit& y) { return hit_order(x, y); });
+                    best.resize(q.max_results);
+                }
+            }
+            const double done = ((double)g * tiles + (double)t1) / ((double)ngroups * tiles);
+            processed.store((int64_t)(done * (double)W * (double)H));
+            progress.store(1 + (int32_t)(done * 78));
+            t0 = t1;
+        }
+    }
+
+    // Exact counts of every centre whose window holds a rare redraw chunk.
+    if (nrare) {
+        FixArgs f{};
+        f.area_x0 = area_x0;
+        f.area_z0 = area_z0;
+        f.width = W;
+        f.height = H;
+        f.rd_min_sq = q.rd_min * q.rd_min;
+        f.center_x = q.center_x;
+        f.center_z = q.center_z;
+        f.min_size = q.min_size;
+        f.max_size = q.max_size;
+        f.fixed = fixed.ptr;
+        f.fixed_count = counters.ptr + 1;
+        f.cap = fixed.count;
+        f.error = flags.ptr + 1;
+        if ((e = cudaMemsetAsync(counters.ptr + 1, 0, 8, stream)) != cudaSuccess ||
+            (e = launch_fixup(rare.ptr, (int32_t)nrare, q.seed, f, stream)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(pinned, counters.ptr + 1, 8, cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
+            (e = cudaMemcpyAsync((char*)pinned + 8, flags.ptr, 8, cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
+            (e = cudaStreamSynchronize(stream)) != cudaSuccess) {
+            set_error("fixup", e);
+            return false;
+        }
+        ++last_launches;
+        const uint64_t nf = *(unsigned long long*)pinned;
+        const uint32_t* fl = (const uint32_t*)((char*)pinned + 8);
+        if (nf > fixed.count || fl[1]) { set_error("fixup overflow", cudaErrorUnknown); return false; }
+        if (nf) {
+            const size_t old = best.size();
+            best.resize(old + nf);
+            if ((e = cudaMemcpyAsync(best.data() + old, fixed.ptr, nf * sizeof(Hit), cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
+                (e = cudaStreamSynchronize(stream)) != cudaSuccess) {
+                set_error("copy", e);
+                return false;
+            }
+            for (size_t i = old; i < best.size(); ++i) ++h[best[i].count];
+        }
+    }
+    if ((e = cudaMemcpyAsync(pinned, flags.ptr, 4, cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(stream)) != cudaSuccess) {
+        set_error("flags", e);
+        return false;
+    }
+    if (*(uint32_t*)pinned) {
+        // A 4-row strip too dense for the byte-lane box: redo the search with the general scan.
+        band_fallbacks++;
+        std::fill(h.begin(), h.end(), 0u);
+        best.clear();
+        return scan_general(q, best, h, cancelled);
+    }
+    return true;
+}
+
+}  // namespace slime

@@ -60,6 +60,17 @@ inline size_t hit_capacity(int32_t max_results) {
     return k > (4u << 20) ? k : (4u << 20);
 }
 
+// Chunk coordinates to the reference's 32-bit block coordinate (wraps like the reference).
+inline int32_t block_of(int32_t c) { return (int32_t)((uint32_t)c * 16u + 8u); }
+
+// Ranking order of the reference: size desc, block x asc, block z asc (SlimeCoreGPU.cu:213-220).
+inline bool hit_order(const Hit& a, const Hit& b) {
+    if (a.count != b.count) return a.count > b.count;
+    const int32_t ax = block_of(a.cx), bx = block_of(b.cx);
+    if (ax != bx) return ax < bx;
+    return block_of(a.cz) < block_of(b.cz);
+}
+
 bool validate_search(int64_t rd_max, int32_t min_size, int32_t max_size, int64_t rd_min,
                      int32_t cx, int32_t cz, const void* results, int32_t max_results);
 
@@ -76,6 +87,19 @@ struct Context {
     DeviceBuffer<unsigned long long> counters;
     DeviceBuffer<unsigned int> hist;
     DeviceBuffer<ExtChunkResult> sites;
+
+    // Band engine: packed row terms, the rare redraw table and the correction buffers.
+    DeviceBuffer<uint32_t> rt;
+    DeviceBuffer<uint64_t> rare_targets;
+    DeviceBuffer<uint32_t> rare_offsets;
+    DeviceBuffer<int2> rare;
+    DeviceBuffer<Hit> fixed;
+    DeviceBuffer<unsigned int> flags;  // [0] overflow, [1] fix-up error, [2] rare count
+    bool band_ready = false;
+    int32_t engine_override = 0;       // 0 auto, 1 general scan, 2 band engine
+    int32_t band_min_threshold = 40;   // auto mode uses the band engine from this threshold
+    int64_t last_rare = 0;             // rare redraw chunks found by the last band search
+    int64_t band_fallbacks = 0;        // band searches redone by the general scan
 
     // Y-scan configuration (set_y_scan_config) and the tables built from it.
     int32_t y_enabled = 0, platform_y = -64, y_min = -64, y_max = 64, y_step = 4;
@@ -104,6 +128,10 @@ struct Context {
 
     bool scan_general(const SearchSpec& q, std::vector<Hit>& best, std::vector<uint32_t>& hist_out,
                       bool& cancelled);
+    bool ensure_band();
+    bool band_eligible(const SearchSpec& q) const;
+    bool scan_band(const SearchSpec& q, std::vector<Hit>& best, std::vector<uint32_t>& hist_out,
+                   bool& cancelled);
     bool score(int64_t seed, ExtChunkResult* host, int32_t n, int32_t scan_xz, bool pack);
     int64_t search(const SearchSpec& q, ExtChunkResult* results);
 };

@@ -2,6 +2,8 @@
 #pragma once
 
 #include <cstdint>
+#include <vector>
+
 #include <cuda_runtime.h>
 
 #include "slime_core.cuh"
@@ -58,5 +60,64 @@ cudaError_t launch_weight_table(uint16_t* weights, const int16_t* outer, const i
 // Fills out[i] = is_slime(seed, x[i], z[i]).
 cudaError_t launch_predicate(int64_t seed, const int64_t* x, const int64_t* z, uint8_t* out,
                              int64_t n, cudaStream_t s);
+
+// ---- band engine (scan_band.cu) ------------------------------------------------------------
+
+// One launch of the band engine over tiles [tile_begin, tile_end) of one band group.
+// The phase axis (u) is x, or z when `transposed`; the band axis (v) is the other one.
+struct BandArgs {
+    const uint64_t* ct;      // column terms (phase axis, no seed), ncols = width_u + 16 entries
+    int64_t ncols;
+    const uint32_t* rt;      // packed row terms (see row_terms_kernel), vrows x rstride
+    int32_t rstride;
+    int32_t vrows;           // base input rows = vbase + 16
+    int32_t vbase;           // base centre rows = min(2^17, height_v)
+    int32_t ubase;           // base centre columns owned = min(2^17, width_u)
+    int64_t width_u, height_v;
+    int32_t j0, nb;          // first band of the group and bands in it (<= 32)
+    int32_t u_tiles, v_tiles;
+    int32_t band_h;
+    int64_t tile_begin, tile_end;
+    int32_t min_size, max_size;
+    int64_t rd_min_sq;
+    int32_t area_x0, area_z0, center_x, center_z;
+    int32_t transposed;
+    Hit* out;
+    uint64_t cap;
+    unsigned long long* emitted;
+    unsigned int* overflow;
+};
+
+size_t band_smem_bytes();
+int band_tile_out_w();
+int band_max_bands();
+cudaError_t band_prepare();
+cudaError_t launch_band_scan(const BandArgs& a, int grid, cudaStream_t s);
+cudaError_t launch_band_terms(uint64_t* ct, int32_t col_first, int32_t ncols, uint32_t* rt,
+                              int32_t rstride, int32_t vrows, int32_t nj, int32_t row_first,
+                              int64_t row_limit, int64_t seed, bool transposed, cudaStream_t s);
+
+// ---- rare redraw correction (rare_fix.cu) ------------------------------------------------
+
+struct FixArgs {
+    int32_t area_x0, area_z0;
+    int64_t width, height;
+    int64_t rd_min_sq;
+    int32_t center_x, center_z;
+    int32_t min_size, max_size;
+    Hit* fixed;
+    unsigned long long* fixed_count;
+    uint64_t cap;
+    unsigned int* error;
+};
+
+void rare_target_table(std::vector<uint64_t>& targets, std::vector<uint32_t>& offsets);
+cudaError_t launch_rare_scan(const uint64_t* targets, const uint32_t* offsets, int64_t seed,
+                             int32_t z_first, int32_t nz, int32_t x_first, int32_t nx, int2* out,
+                             uint32_t cap, unsigned int* count, cudaStream_t s);
+cudaError_t launch_fixup(const int2* rare, int32_t nrare, int64_t seed, const FixArgs& f,
+                         cudaStream_t s);
+cudaError_t launch_filter_hits(Hit* hits, int64_t n, const int2* rare, int32_t nrare,
+                               cudaStream_t s);
 
 }  // namespace slime

@@ -4,7 +4,7 @@
 // and bf16 figures, so the INT32 peak is measured here, on the same device and clocks as the
 // scan. Each probe runs independent dependency chains (8 per thread) of one instruction form
 // over a full grid and reports lane operations per second. Kinds:
-//   0 LOP3 (3-input logic)        1 IADD3 (3-input add)     2 IMAD (multiply-add)
+//   0 LOP3 (3-input logic)        1 IADD3 + LOP3 (2 adds, 1 xor) 2 IMAD (multiply-add)
 //   3 POPC                        4 mixed generator step: IADD3 + LOP3 + IMAD + ISETP + VOTE
 //   5 b1 tensor AND+POPC, mma.sync m16n8k256 (reported as 32-bit AND+POPC lane-ops: 1024 per mma)
 //   6 SHF (funnel shift)
@@ -47,8 +47,10 @@ __global__ void __launch_bounds__(kTpb) probe_kernel(uint32_t* sink, int iters, 
                     asm volatile("lop3.b32 %0, %0, %1, %2, 0x96;" : "+r"(x) : "r"(k0), "r"(k1));
                     asm volatile("lop3.b32 %0, %0, %1, %2, 0x78;" : "+r"(x) : "r"(k1), "r"(k0));
                 } else if constexpr (KIND == 1) {
-                    asm volatile("{ .reg .u32 t; add.u32 t, %0, %1; add.u32 %0, t, %2; }" : "+r"(x) : "r"(k0), "r"(k1));
-                    asm volatile("{ .reg .u32 t; add.u32 t, %0, %1; sub.u32 %0, t, %2; }" : "+r"(x) : "r"(k1), "r"(k0));
+                    // Three-input adds whose operands change every step (no invariant folding).
+                    const uint32_t y = v[(c + 1) % kChains], w = v[(c + 3) % kChains];
+                    x = x + y + w;
+                    x = x + w + (y ^ k0);
                 } else if constexpr (KIND == 2) {
                     asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(x) : "r"(k0), "r"(k1));
                     asm volatile("mad.lo.u32 %0, %0, %1, %2;" : "+r"(x) : "r"(k1), "r"(k0));
@@ -113,7 +115,7 @@ extern "C" int32_t slime_b200_microbench(int32_t kind, int32_t iters, double* la
     double per_iter_thread;  // lane operations per thread per iteration
     switch (kind) {
         case 0: e = run<0>(blocks, iters, &ms); per_iter_thread = 2.0 * kChains; break;
-        case 1: e = run<1>(blocks, iters, &ms); per_iter_thread = 2.0 * kChains; break;
+        case 1: e = run<1>(blocks, iters, &ms); per_iter_thread = 3.0 * kChains; break;
         case 2: e = run<2>(blocks, iters, &ms); per_iter_thread = 2.0 * kChains; break;
         case 3: e = run<3>(blocks, iters, &ms); per_iter_thread = 2.0 * kChains; break;
         case 4: e = run<4>(blocks, iters, &ms); per_iter_thread = 5.0 * kChains; break;

@@ -51,6 +51,8 @@ SIGNATURES = {
     "slime_b200_last_error": (C.c_char_p, []),
     "slime_b200_last_search_stats": (None, [C.POINTER(C.c_double), C.POINTER(i64)]),
     "slime_b200_is_slime_batch": (i32, [i64, vp, vp, u8p, i64]),
+    "slime_b200_last_rare_chunks": (i64, []),
+    "slime_b200_set_engine": (None, [i32, i32]),
     "slime_b200_microbench": (i32, [i32, i32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
 }
 

@@ -1,0 +1,127 @@
+"""GPU parity of the band engine (shared-LCG generator + rare redraw correction).
+
+The band engine must return exactly what the general scan, the oracle and the reference return:
+same totals, same ranked records."""
+import numpy as np
+import pytest
+
+from oracle.oracle import REF_GPU_SO, python_is_slime
+
+pytestmark = pytest.mark.gpu
+
+M48 = (1 << 48) - 1
+M64 = (1 << 64) - 1
+LCG = 0x5DEECE66D
+LCG_INV = pow(LCG, -1, 1 << 48)
+SCRAMBLE = 0x3AD8025F
+
+
+def s32(v):
+    v &= 0xFFFFFFFF
+    return v - (1 << 32) if v & 0x80000000 else v
+
+
+def mix_terms(x, z):
+    x, z = s32(x), s32(z)
+    return (s32(x * x * 0x4C1906) + s32(x * 0x5AC0DB) + s32(z * z) * 0x4307A7 + s32(z * 0x5F24F)) & M64
+
+
+def rare_seed(x, z, k=0):
+    """A world seed whose chunk (x, z) has a rejected first draw and is a slime chunk after
+    Java's redraw (one of the 104,848 rare states; k picks which)."""
+    found = 0
+    for s1 in range((1 << 48) - (1 << 20), 1 << 48):
+        st = s1
+        while True:
+            st = (st * LCG + 0xB) & M48
+            bits = st >> 17
+            if bits < 2147483640:
+                break
+        if bits % 10 == 0:
+            if found == k:
+                state0 = (LCG_INV * (s1 - 0xB)) & M48
+                mix = (state0 ^ SCRAMBLE ^ LCG) & M48 | (0x1234 << 48)
+                seed = (mix - mix_terms(x, z)) & M64
+                return seed - (1 << 64) if seed >> 63 else seed
+            found += 1
+
+
+@pytest.fixture(scope="module")
+def core():
+    from slime_b200 import build
+    from slime_b200.lib import SlimeCoreB200
+    build.build()
+    c = SlimeCoreB200()
+    c.set_y_scan_config(0, -64, -64, 64, 4)
+    yield c
+    c.lib.slime_b200_set_engine(0, 0)
+
+
+def run(core, mode, *args, **kw):
+    core.lib.slime_b200_set_engine(mode, 0)
+    core.lib.reset_cancel()
+    try:
+        return core.search(*args, **kw)
+    finally:
+        core.lib.slime_b200_set_engine(0, 0)
+
+
+@pytest.mark.parametrize("idx", [0, 1, 2, 7])
+def test_band_engine_search_golden(core, golden, idx):
+    g = golden["search"]
+    name = str(g["names"][idx])
+    seed, rd_max, lo, hi, rd_min, cx, cz, maxr, total = (int(v) for v in g["params"][idx])
+    assert lo >= 28
+    got_total, got = run(core, 2, seed, rd_max, lo, hi, rd_min, cx, cz, maxr)
+    assert core.lib.get_gpu_v1_algorithm() == 200
+    assert got_total == total, name
+    assert np.array_equal(got, g[f"{name}_results"]), name
+
+
+@pytest.mark.parametrize("k,thr", [(0, 30), (1, 28), (2, 33), (3, 29)])
+def test_band_engine_planted_rare_chunk(core, oracle, k, thr):
+    x, z = 123_457 + 17 * k, -98_765 - 11 * k
+    seed = rare_seed(x, z, k)
+    assert python_is_slime(seed, x, z)
+    args = (seed, 60, thr, 221, 0, x + 5, z - 3, 5000)
+    t_o, r_o = oracle.search(*args)
+    t_b, r_b = run(core, 2, *args)
+    assert core.lib.slime_b200_last_rare_chunks() >= 1
+    assert t_b == t_o
+    assert np.array_equal(r_b, r_o)
+    # The rare chunk must matter: some centre's count differs from the first-draw count.
+    t_g, r_g = run(core, 1, *args)
+    assert t_g == t_o and np.array_equal(r_g, r_o)
+
+
+def test_band_engine_planted_rare_upper_bound(core, oracle):
+    x, z = -1_500_000, 1_400_000
+    seed = rare_seed(x, z, 5)
+    args = (seed, 40, 30, 34, 7, x, z, 2000)
+    t_o, r_o = oracle.search(*args)
+    t_b, r_b = run(core, 2, *args)
+    assert t_b == t_o and np.array_equal(r_b, r_o)
+
+
+@pytest.mark.parametrize("case", [
+    (20240607, 140_000, 54, 221, 0, 0, 0, 2000),          # 2 phases x 3 bands, wide tiles
+    (-31337, 300_000, 57, 221, 0, 400_000, -250_000, 500),  # 5 x 5 periods, offset centre
+    (77, 270_000, 50, 60, 90_000, -1_000_000, 1_000_000, 3000),  # upper bound + annulus
+])
+def test_band_vs_general_medium(core, case):
+    t_g, r_g = run(core, 1, *case)
+    t_b, r_b = run(core, 2, *case)
+    assert t_b == t_g
+    assert np.array_equal(r_b, r_g)
+
+
+@pytest.mark.skipif(not REF_GPU_SO.exists(), reason="reference GPU library not built")
+def test_band_full_world_vs_reference_gpu(core):
+    from oracle.oracle import RefGpu
+    from slime_b200 import workloads
+    spec = workloads.full_world_scan()
+    t_b, r_b = run(core, 0, spec.seed, spec.radius, 60, 221, 0, 0, 0, 1000)
+    assert core.lib.get_gpu_v1_algorithm() == 200
+    t_r, r_r = RefGpu().search(spec.seed, spec.radius, 60, 221, 0, 0, 0, 1000)
+    assert t_b == t_r
+    assert np.array_equal(r_b, r_r)
