@@ -124,6 +124,10 @@ int64_t slime_b200_last_rare_chunks(void);
  * identical either way; only speed differs. */
 void slime_b200_set_engine(int32_t mode, int32_t band_min_threshold);
 
+/* Generator variant of the band engine (results are identical): band_mad_add != 0 issues the
+ * per-band add on the multiply pipe instead of the integer ALU. */
+void slime_b200_set_tuning(int32_t band_mad_add);
+
 /* Last CUDA error text of this library ("" if none). */
 const char* slime_b200_last_error(void);
 
@@ -134,7 +138,8 @@ int32_t slime_b200_is_slime_batch(int64_t seed, const int64_t* x, const int64_t*
 
 /* Integer-pipe throughput probe on the current device (the denominator of the scan's roofline).
  * kind: 0 LOP3, 1 IADD3, 2 IMAD, 3 POPC, 4 generator mix (IADD3+LOP3+IMAD+ISETP+VOTE),
- * 5 b1 tensor AND+POPC (mma.sync m16n8k256), 6 SHF. Writes lane operations per second and the
+ * 5 b1 tensor AND+POPC (mma.sync m16n8k256), 6 SHF, 7 ISETP+VOTE+LOP3, 8 generator mix with the
+ * add as a multiply-add. Writes lane operations per second and the
  * timed milliseconds. Returns 0, or -1 on a CUDA failure. */
 int32_t slime_b200_microbench(int32_t kind, int32_t iters, double* lane_ops_per_s, double* ms);
 

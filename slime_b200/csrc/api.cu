@@ -527,6 +527,11 @@ void slime_b200_last_search_stats(double* kernel_ms, int64_t* launches) {
 
 int64_t slime_b200_last_rare_chunks(void) { return ctx().last_rare; }
 
+void slime_b200_set_tuning(int32_t band_mad_add) {
+    std::lock_guard<std::mutex> lock(ctx().mu);
+    ctx().band_mad_add = band_mad_add ? 1 : 0;
+}
+
 void slime_b200_set_engine(int32_t mode, int32_t band_min_threshold) {
     std::lock_guard<std::mutex> lock(ctx().mu);
     ctx().engine_override = (mode >= 0 && mode <= 2) ? mode : 0;

@@ -137,6 +137,8 @@ bool Context::scan_band(const SearchSpec& q, std::vector<Hit>& best, std::vector
             a.cap = cap;
             a.emitted = counters.ptr;
             a.overflow = flags.ptr;
+            a.one = 1u;
+            a.mad_add = band_mad_add;
             const auto c0 = std::chrono::steady_clock::now();
             if ((e = cudaMemsetAsync(counters.ptr, 0, 8, stream)) != cudaSuccess ||
                 (e = cudaEventRecord(ev_a, stream)) != cudaSuccess ||

@@ -86,6 +86,8 @@ struct BandArgs {
     uint64_t cap;
     unsigned long long* emitted;
     unsigned int* overflow;
+    uint32_t one;            // the value 1 (run time): band adds as multiply-adds when mad_add
+    int32_t mad_add;
 };
 
 size_t band_smem_bytes();

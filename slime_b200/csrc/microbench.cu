@@ -7,7 +7,8 @@
 //   0 LOP3 (3-input logic)        1 IADD3 + LOP3 (2 adds, 1 xor) 2 IMAD (multiply-add)
 //   3 POPC                        4 mixed generator step: IADD3 + LOP3 + IMAD + ISETP + VOTE
 //   5 b1 tensor AND+POPC, mma.sync m16n8k256 (reported as 32-bit AND+POPC lane-ops: 1024 per mma)
-//   6 SHF (funnel shift)
+//   6 SHF (funnel shift)          7 ISETP + VOTE + LOP3
+//   8 generator step with the add issued as a multiply-add (IMAD + LOP3 + IMAD + ISETP + VOTE)
 #include <cuda_runtime.h>
 
 #include <cstdint>
@@ -70,6 +71,26 @@ __global__ void __launch_bounds__(kTpb) probe_kernel(uint32_t* sink, int iters, 
                         "vote.sync.ballot.b32 %1, p, 0xffffffff; }"
                         : "+r"(x), "+r"(bal[c])
                         : "r"(k0), "r"(k1));
+                } else if constexpr (KIND == 7) {
+                    // compare + ballot only
+                    asm volatile(
+                        "{ .reg .pred p;\n"
+                        "setp.lt.u32 p, %0, %2;\n"
+                        "vote.sync.ballot.b32 %1, p, 0xffffffff; }"
+                        : "+r"(x), "+r"(bal[c])
+                        : "r"(k0));
+                    x ^= bal[c];
+                } else if constexpr (KIND == 8) {
+                    // generator step with the add as a multiply-add by a run-time 1 (k1 == 1 here)
+                    asm volatile(
+                        "{ .reg .pred p; .reg .u32 t, h;\n"
+                        "mad.lo.u32 t, %1, %3, %0;\n"
+                        "xor.b32 h, t, 0x2F21A;\n"
+                        "mad.lo.u32 %0, h, 0xC6D4F14B, %2;\n"
+                        "setp.lt.u32 p, %0, 858993456;\n"
+                        "vote.sync.ballot.b32 %1, p, 0xffffffff; }"
+                        : "+r"(x), "+r"(bal[c])
+                        : "r"(k0), "r"(k1));
                 } else if constexpr (KIND == 6) {
                     asm volatile("shf.r.wrap.b32 %0, %0, %1, %2;" : "+r"(x) : "r"(k0), "r"(k1));
                     asm volatile("shf.l.wrap.b32 %0, %1, %0, %2;" : "+r"(x) : "r"(k1), "r"(k0));
@@ -93,7 +114,7 @@ cudaError_t run(int blocks, int iters, float* ms) {
     cudaEventCreate(&b);
     probe_kernel<KIND><<<blocks, kTpb>>>(sink, iters / 8 + 1, 3u, 5u);  // warm-up
     cudaEventRecord(a);
-    probe_kernel<KIND><<<blocks, kTpb>>>(sink, iters, 0x9E3779B9u, 0x7F4A7C15u);
+    probe_kernel<KIND><<<blocks, kTpb>>>(sink, iters, 0x9E3779B9u, KIND == 8 ? 1u : 0x7F4A7C15u);
     cudaEventRecord(b);
     e = cudaEventSynchronize(b);
     cudaEventElapsedTime(ms, a, b);
@@ -121,6 +142,8 @@ extern "C" int32_t slime_b200_microbench(int32_t kind, int32_t iters, double* la
         case 4: e = run<4>(blocks, iters, &ms); per_iter_thread = 5.0 * kChains; break;
         case 5: e = run<5>(blocks, iters, &ms); per_iter_thread = 4.0 * 1024.0 / 32.0; break;
         case 6: e = run<6>(blocks, iters, &ms); per_iter_thread = 2.0 * kChains; break;
+        case 7: e = run<7>(blocks, iters, &ms); per_iter_thread = 3.0 * kChains; break;
+        case 8: e = run<8>(blocks, iters, &ms); per_iter_thread = 5.0 * kChains; break;
         default: return -1;
     }
     if (e != cudaSuccess) return -1;

@@ -9,12 +9,17 @@
 //    position the low-17-bit work (carry, Q, D, parity) is done once; per band it costs one add,
 //    one xor, one multiply-add, one compare and one ballot for the two phases together, because
 //    the parity tells which of the two phases can be a first-draw slime chunk.
-//  * Ballots land in a 20-row shared ring (one plane per band plus the phase-swap plane).
-//  * Counting is SWAR in byte lanes on 4x4 centre groups: nibble popcounts of 4 rows give 4x4
-//    block counts, three funnel shifts and two adds give the 20-column sums of 8 groups per word,
-//    and a rolling sum over 5 row batches gives the 20x20 box that bounds the 16 circles. Groups
-//    whose box reaches the threshold get exact 221-cell counts from the ring (one popcount per
-//    window row, spread over the whole CTA), and those in range are appended to the hit list.
+//  * Rows advance in batches of 4. Ballots of a batch go to one of two 4-row buffers, so one
+//    barrier per batch separates the generator (batch b+1) from the counter (batch b).
+//  * Counting is SWAR in byte lanes on 4x4 centre groups. A warp owns a combo (phase, band) row
+//    with one lane per 32-column word: nibble popcounts of the 4 rows give 4x4 block counts,
+//    the neighbour word comes by shuffle, three funnel shifts and two adds give the 20-column
+//    strip sums of the word's 8 groups, and a rolling sum over 5 batches gives the 20x20 box of
+//    each group, which bounds its 16 windows. A flagged group is re-tested in registers with
+//    the 32 cells of rows 0, 1, 18 and 19 that lie outside every window removed (368 cells).
+//  * Groups that pass both go to a queue; the CTA re-evaluates queued groups from the term
+//    tables (one warp per group: 20 x 20 first-draw bits, 16 exact window counts) and appends
+//    the centres in range to the hit list.
 #include "band_math.cuh"
 #include "engine.h"
 
@@ -24,29 +29,29 @@ namespace {
 using namespace band;
 
 constexpr int kTpb = 512;
+constexpr int kWarps = kTpb / 32;
 constexpr int kWords = 32;                  // words per ring row: 1,024 base columns
 constexpr int kOutW = kWords * 32 - 16;     // 1,008 centres per tile row
 constexpr int kMaxBands = 32;
 constexpr int kSwPlane = kMaxBands;         // plane of the phase-swap ballot
-constexpr int kPlanes = kMaxBands + 4;      // 16-byte aligned rows of planes
-constexpr int kRing = 20;                   // rows in the ring (5 batches of 4)
+constexpr int kPlanes = kMaxBands + 4;      // 16-byte aligned word records
 constexpr int kMaxCombos = 2 * kMaxBands;
-constexpr int kMaxPairs = kMaxCombos * kWords;
-constexpr int kSlots = kMaxPairs / kTpb;    // (combo, word) pairs per thread
-constexpr int kSurvCap = 192;               // survivor groups processed per round
+constexpr int kSlots = kMaxCombos / kWarps; // combo rows counted per warp
+constexpr int kQueueCap = 1024;
+constexpr int kQueueFlush = 512;
 constexpr unsigned kFull = 0xFFFFFFFFu;
 
 struct __align__(16) BandSmem {
-    uint32_t ring[kRing][kWords + 1][kPlanes];   // word kWords is a zero pad
-    uint32_t hist_e[5][kMaxPairs];
-    uint32_t hist_o[5][kMaxPairs];
-    uint32_t eo_e[kMaxCombos][kWords + 1];
-    uint32_t eo_o[kMaxCombos][kWords + 1];
-    uint32_t rows[4][kMaxBands + 1];             // batch row terms: [0] low 17 bits, [1+m] high
-    uint32_t surv[kSurvCap];                     // (pair << 3) | group
-    int cnt[kSurvCap * 16];
-    int nsurv;
-    int any;
+    uint32_t ring[2][4][kWords][kPlanes];     // [buffer][row][word][band planes | swap plane]
+    uint32_t hist_e[5][kMaxCombos][kWords];   // strip sums of the last 5 batches (even groups)
+    uint32_t hist_o[5][kMaxCombos][kWords];   // (odd groups)
+    uint32_t hist_n[5][kMaxCombos][kWords];   // nibble counts of rows 0+1 of the last 5 batches
+    uint32_t rows[3][4][kMaxBands + 1];       // row terms of 3 batches: [0] low 17, [1+m] high
+    uint32_t rvalid[3][4];                    // bit m: the row exists in band m
+    uint32_t queue[kQueueCap];                // combo << 24 | word << 19 | group << 16 | batch
+    uint32_t scratch[kWarps][20];             // re-evaluation rows, one block per warp
+    int qcount;
+    int qover;
 };
 
 __device__ __forceinline__ uint32_t nibble_counts(uint32_t r) {
@@ -54,232 +59,331 @@ __device__ __forceinline__ uint32_t nibble_counts(uint32_t r) {
     return (a & 0x33333333u) + ((a >> 2) & 0x33333333u);
 }
 
-// Maps the per-byte "reached" bits of the even (te) and odd (to) group sums to an 8-bit mask.
-__device__ __forceinline__ uint32_t group_mask(uint32_t te, uint32_t to) {
-    uint32_t m = 0;
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        m |= ((te >> (8 * k + 7)) & 1u) << (2 * k);
-        m |= ((to >> (8 * k + 7)) & 1u) << (2 * k + 1);
-    }
-    return m;
+// Per byte: high bit set where v >= t (v, t < 256; borrow-free because v | 0x80 >= 128 >= t').
+// Bytes >= 128 always report (a superset is safe: flagged groups are re-tested).
+__device__ __forceinline__ uint32_t bytes_at_least(uint32_t v, uint32_t t4) {
+    return (((v | 0x80808080u) - t4) | v) & 0x80808080u;
 }
 
+// Appends the groups of `gm` to the queue; returns those that did not fit (kept pending).
+__device__ __forceinline__ uint32_t push_groups(BandSmem& S, int combo, int word, uint32_t gm, int b) {
+    while (gm) {
+        const int g = __ffs(gm) - 1;
+        const int idx = atomicAdd(&S.qcount, 1);
+        if (idx >= kQueueCap) {
+            S.qover = 1;
+            return gm;
+        }
+        S.queue[idx] = ((uint32_t)combo << 24) | ((uint32_t)word << 19) | ((uint32_t)g << 16) | (uint32_t)b;
+        gm &= gm - 1;
+    }
+    return 0;
+}
+
+struct Tile {
+    int u0, v0, i0, out_h;
+};
+
+// Re-evaluates the queued groups from the term tables and appends the centres in range.
+__device__ void flush_queue(BandSmem& S, const BandArgs& a, const Tile& T, int warp, int lane) {
+    const int n = min(S.qcount, kQueueCap);
+    const bool no_upper = a.max_size >= 221;
+    for (int s = warp; s < n; s += kWarps) {
+        const uint32_t rec = S.queue[s];
+        const int combo = (int)(rec >> 24), word = (int)((rec >> 19) & 31);
+        const int g = (int)((rec >> 16) & 7), b = (int)(rec & 0xFFFF);
+        const int ph = combo & 1, m = combo >> 1;
+        const int c0 = word * 32 + 4 * g;       // first window column (tile-relative input col)
+        const int r0 = 4 * (b - 4);             // first window row (tile-relative input row)
+        uint64_t xt = 0;
+        if (lane < 20) {
+            const int64_t idx = (int64_t)T.u0 + c0 + lane + (int64_t)(T.i0 + ph) * kPeriod;
+            xt = idx < a.ncols ? a.ct[idx] : 0;
+        }
+        for (int t = 0; t < 20; ++t) {
+            const int vi = T.v0 + r0 + t;
+            uint64_t zt = 0;
+            if (vi < a.vrows) {
+                const uint32_t* row = a.rt + (int64_t)vi * a.rstride;
+                zt = (uint64_t)row[0] | ((uint64_t)row[1 + a.j0 + m] << kPeriodBits);
+            }
+            const uint32_t bits = __ballot_sync(kFull, lane < 20 && first_draw_slime(xt, zt));
+            if (lane == 0) S.scratch[warp][t] = bits;
+        }
+        __syncwarp();
+        bool keep = false;
+        int count = 0, cx = 0, cz = 0;
+        if (lane < 16) {
+            const int dx = lane & 3, dz = lane >> 2;
+#pragma unroll
+            for (int i = 0; i < 17; ++i)
+                count += __popc((S.scratch[warp][dz + i] >> dx) & window_row_mask(i));
+            const int c = c0 + dx, rr = r0 + dz;
+            const int64_t u = (int64_t)T.u0 + c, v = (int64_t)T.v0 + rr;
+            const int64_t cu = u + (int64_t)(T.i0 + ph) * kPeriod;
+            const int64_t cv = v + (int64_t)(a.j0 + m) * kPeriod;
+            keep = count >= a.min_size && (no_upper || count <= a.max_size) && c < kOutW &&
+                   u < a.ubase && rr < T.out_h && cu < a.width_u && cv < a.height_v;
+            if (keep) {
+                cx = (int32_t)(a.transposed ? a.area_x0 + cv : a.area_x0 + cu);
+                cz = (int32_t)(a.transposed ? a.area_z0 + cu : a.area_z0 + cv);
+                if (a.rd_min_sq) {
+                    const int64_t ddx = (int64_t)cx - a.center_x, ddz = (int64_t)cz - a.center_z;
+                    keep = ddx * ddx + ddz * ddz >= a.rd_min_sq;
+                }
+            }
+        }
+        const unsigned mk = __ballot_sync(kFull, keep);
+        if (mk) {
+            unsigned long long base = 0;
+            if (lane == 0) base = atomicAdd(a.emitted, (unsigned long long)__popc(mk));
+            base = __shfl_sync(kFull, base, 0);
+            if (keep) {
+                const unsigned long long idx = base + __popc(mk & ((1u << lane) - 1u));
+                if (idx < a.cap) a.out[idx] = Hit{count, cx, cz};
+            }
+        }
+        __syncwarp();
+    }
+}
+
+// Processes the queue (all threads; block-uniform entry) and re-pushes pending groups. With
+// `final` it repeats until queue and pending groups are empty; otherwise it may return with a
+// partial queue (fewer than kQueueFlush groups) and no pending groups.
+__device__ void drain_queue(BandSmem& S, const BandArgs& a, const Tile& T, int tid, int warp,
+                            int lane, uint32_t (&pend)[kSlots], int (&pend_b)[kSlots], bool final) {
+    for (;;) {
+        flush_queue(S, a, T, warp, lane);
+        __syncthreads();
+        if (tid == 0) { S.qcount = 0; S.qover = 0; }
+        __syncthreads();
+        bool left = false;
+#pragma unroll
+        for (int k = 0; k < kSlots; ++k) {
+            if (pend[k]) pend[k] = push_groups(S, warp + kWarps * k, lane, pend[k], pend_b[k]);
+            left |= pend[k] != 0;
+        }
+        const bool more = __syncthreads_or(left);
+        const int queued = S.qcount;  // stable: every push precedes the barrier above
+        if (more) continue;
+        if (queued == 0 || (!final && queued < kQueueFlush)) break;
+    }
+}
+
+template <bool kMadAdd>
 __global__ void __launch_bounds__(kTpb, 1) band_scan_kernel(const BandArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     BandSmem& S = *reinterpret_cast<BandSmem*>(smem_raw);
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int nb = a.nb, ncombo = 2 * nb, npairs = ncombo * kWords;
-    const uint32_t bias = (uint32_t)(128 - a.min_size) * 0x01010101u;
-    const bool no_upper = a.max_size >= 221;
+    const int nb = a.nb, ncombo = 2 * nb;
+    const uint32_t thr4 = (uint32_t)min(a.min_size, 128) * 0x01010101u;
+    const uint32_t one = a.one;  // 1 at run time: keeps the band add on the multiply pipe
     uint32_t guard = 0;
-
-    // Zero pads that are never written: ring word kWords and the E/O pad word.
-    for (int i = tid; i < kRing * kPlanes; i += kTpb) S.ring[i / kPlanes][kWords][i % kPlanes] = 0;
-    for (int i = tid; i < kMaxCombos; i += kTpb) {
-        S.eo_e[i][kWords] = 0;
-        S.eo_o[i][kWords] = 0;
-    }
+    if (tid == 0) { S.qcount = 0; S.qover = 0; }
 
     for (int64_t tile = a.tile_begin + blockIdx.x; tile < a.tile_end; tile += gridDim.x) {
+        Tile T;
         const int ut = (int)(tile % a.u_tiles);
         const int64_t rest = tile / a.u_tiles;
         const int vt = (int)(rest % a.v_tiles);
-        const int pp = (int)(rest / a.v_tiles);
-        const int i0 = 2 * pp;
-        const int u0 = ut * kOutW;
-        const int v0 = vt * a.band_h;
-        const int out_h = min(a.band_h, a.vbase - v0);
-        const int batches = (out_h + 16 + 3) / 4;
+        T.i0 = 2 * (int)(rest / a.v_tiles);
+        T.u0 = ut * kOutW;
+        T.v0 = vt * a.band_h;
+        // Tiles with no centre of the area in any of their combos are skipped (block-uniform).
+        if ((int64_t)T.u0 + (int64_t)T.i0 * kPeriod >= a.width_u ||
+            (int64_t)T.v0 + (int64_t)a.j0 * kPeriod >= a.height_v)
+            continue;
+        T.out_h = min(a.band_h, a.vbase - T.v0);
+        const int batches = (T.out_h + 16 + 3) / 4;
 
-        // Column terms of this thread's two generator words, for phases i0 and i0 + 1.
+        // Generator columns of this thread: words 2*warp and 2*warp+1, lane = bit.
         uint32_t lox[2], xh0[2], xh1[2];
 #pragma unroll
         for (int k = 0; k < 2; ++k) {
-            const int64_t idx0 = (int64_t)u0 + (warp * 2 + k) * 32 + lane + (int64_t)i0 * kPeriod;
+            const int64_t idx0 = (int64_t)T.u0 + (warp * 2 + k) * 32 + lane + (int64_t)T.i0 * kPeriod;
             const uint64_t x0 = idx0 < a.ncols ? a.ct[idx0] : 0;
             const uint64_t x1 = idx0 + kPeriod < a.ncols ? a.ct[idx0 + kPeriod] : 0;
             lox[k] = (uint32_t)x0 & 0x1FFFFu;
             xh0[k] = (uint32_t)(x0 >> kPeriodBits);
             xh1[k] = (uint32_t)(x1 >> kPeriodBits);
         }
-        uint32_t re[kSlots], ro[kSlots];
+        // Counter slots of this warp: combo rows warp + 16*k; lane = word. Columns of the word
+        // that exist for the slot's phase (bits beyond are masked to zero before counting).
+        uint32_t cm[kSlots], fx[kSlots], re[kSlots], ro[kSlots], pend[kSlots];
+        int pend_b[kSlots];
 #pragma unroll
-        for (int k = 0; k < kSlots; ++k) re[k] = ro[k] = 0;
-        for (int i = tid; i < 5 * kMaxPairs; i += kTpb) {
-            (&S.hist_e[0][0])[i] = 0;
-            (&S.hist_o[0][0])[i] = 0;
+        for (int k = 0; k < kSlots; ++k) {
+            const int combo = warp + kWarps * k;
+            const int64_t first = (int64_t)T.u0 + lane * 32 + (int64_t)(T.i0 + (combo & 1)) * kPeriod;
+            const int64_t nvalid = a.ncols - first;
+            cm[k] = nvalid >= 32 ? ~0u : nvalid <= 0 ? 0u : (1u << nvalid) - 1u;
+            fx[k] = ((combo ^ (combo >> 1)) & 1) ? 0u : ~0u;
+            re[k] = ro[k] = 0;
+            pend[k] = 0;
+            pend_b[k] = 0;
+        }
+        for (int i = tid; i < 5 * kMaxCombos * kWords; i += kTpb) {
+            (&S.hist_e[0][0][0])[i] = 0;
+            (&S.hist_o[0][0][0])[i] = 0;
+            (&S.hist_n[0][0][0])[i] = 0;
+        }
+        // Row terms of batches 0 and 1.
+        for (int i = tid; i < 2 * 4 * (nb + 1); i += kTpb) {
+            const int bb = i / (4 * (nb + 1)), q = (i / (nb + 1)) % 4, e = i % (nb + 1);
+            const int vi = T.v0 + 4 * bb + q;
+            S.rows[bb][q][e] = vi < a.vrows ? a.rt[(int64_t)vi * a.rstride + (e == 0 ? 0 : a.j0 + e)] : 0u;
+        }
+        if (tid < 8) {
+            const int bb = tid >> 2, q = tid & 3, vi = T.v0 + 4 * bb + q;
+            const int64_t room = a.height_v + 16 - ((int64_t)vi + (int64_t)a.j0 * kPeriod);
+            uint32_t mask = 0;
+            if (vi < a.vrows)
+                for (int m = 0; m < nb; ++m)
+                    if (room - (int64_t)m * kPeriod > 0) mask |= 1u << m;
+            S.rvalid[bb][q] = mask;
         }
         __syncthreads();
 
         for (int b = 0; b < batches; ++b) {
-            // (1) Row terms of the batch's 4 input rows (low 17 bits and the band high parts).
-            for (int i = tid; i < 4 * (nb + 1); i += kTpb) {
-                const int q = i / (nb + 1), e = i % (nb + 1);
-                const int vi = v0 + 4 * b + q;
-                S.rows[q][e] = vi < a.vrows ? a.rt[(int64_t)vi * a.rstride + (e == 0 ? 0 : a.j0 + e)] : 0u;
-            }
-            __syncthreads();
-
-            // (2) Generator: 4 rows x 2 words per warp.
+            const int rb = b % 3, buf = b & 1;
+            // ---- generator: batch b into ring[buf] ------------------------------------------
 #pragma unroll 1
             for (int q = 0; q < 4; ++q) {
-                const int slot = (4 * b + q) % kRing;
-                const uint32_t zlo = S.rows[q][0];
-                const uint32_t zpar = (S.rows[q][1] ^ kXorHi) & 1u;
+                const uint32_t* zr = &S.rows[rb][q][0];
+                const uint32_t zlo = zr[0];
+                const uint32_t zpar = (zr[1] ^ kXorHi) & 1u;
+                uint32_t xa[2], xb[2], dd[2];
 #pragma unroll
                 for (int k = 0; k < 2; ++k) {
-                    const int word = warp * 2 + k;
                     const Shared sh = shared_part(lox[k], zlo);
                     const uint32_t pi = (sh.q0 ^ xh0[k] ^ sh.carry ^ zpar) & 1u;
-                    const uint32_t xa = (pi ? xh1[k] : xh0[k]) + sh.carry;
-                    const uint32_t xb = (pi ? xh0[k] : xh1[k]) + sh.carry;
+                    xa[k] = (pi ? xh1[k] : xh0[k]) + sh.carry;
+                    xb[k] = (pi ? xh0[k] : xh1[k]) + sh.carry;
+                    dd[k] = sh.d;
                     const uint32_t sw = __ballot_sync(kFull, pi != 0);
-                    uint32_t* dst = &S.ring[slot][word][0];
-                    int m = 0;
-                    for (; m + 1 < nb; m += 2) {
-                        const uint32_t ha = ((xa + S.rows[q][1 + m]) ^ kXorHi) * kMulH + sh.d;
-                        const uint32_t hb = ((xb + S.rows[q][2 + m]) ^ kXorHi) * kMulH + sh.d;
-                        const uint32_t wa = __ballot_sync(kFull, ha < kHitBelow);
-                        const uint32_t wb = __ballot_sync(kFull, hb < kHitBelow);
-                        if (lane == 0) *reinterpret_cast<uint2*>(dst + m) = make_uint2(wa, wb);
+                    if (lane == 0) S.ring[buf][q][warp * 2 + k][kSwPlane] = sw;
+                }
+                uint32_t* dst0 = &S.ring[buf][q][warp * 2][0];
+                uint32_t* dst1 = &S.ring[buf][q][warp * 2 + 1][0];
+                auto hit = [&](uint32_t x, uint32_t z, uint32_t d) {
+                    const uint32_t t = kMadAdd ? z * one + x : z + x;
+                    return ((t ^ kXorHi) * kMulH + d) < kHitBelow;
+                };
+                int m = 0;
+                for (; m + 3 < nb; m += 4) {
+                    const uint32_t z0 = zr[1 + m], z1 = zr[2 + m], z2 = zr[3 + m], z3 = zr[4 + m];
+                    const uint32_t a0 = __ballot_sync(kFull, hit(xa[0], z0, dd[0]));
+                    const uint32_t a1 = __ballot_sync(kFull, hit(xa[1], z0, dd[1]));
+                    const uint32_t b0 = __ballot_sync(kFull, hit(xb[0], z1, dd[0]));
+                    const uint32_t b1 = __ballot_sync(kFull, hit(xb[1], z1, dd[1]));
+                    const uint32_t c0 = __ballot_sync(kFull, hit(xa[0], z2, dd[0]));
+                    const uint32_t c1 = __ballot_sync(kFull, hit(xa[1], z2, dd[1]));
+                    const uint32_t e0 = __ballot_sync(kFull, hit(xb[0], z3, dd[0]));
+                    const uint32_t e1 = __ballot_sync(kFull, hit(xb[1], z3, dd[1]));
+                    if (lane == 0) {
+                        *reinterpret_cast<uint4*>(dst0 + m) = make_uint4(a0, b0, c0, e0);
+                        *reinterpret_cast<uint4*>(dst1 + m) = make_uint4(a1, b1, c1, e1);
                     }
-                    if (m < nb) {
-                        const uint32_t ha = ((xa + S.rows[q][1 + m]) ^ kXorHi) * kMulH + sh.d;
-                        const uint32_t wa = __ballot_sync(kFull, ha < kHitBelow);
-                        if (lane == 0) dst[m] = wa;
+                }
+                for (; m < nb; ++m) {
+                    const uint32_t z0 = zr[1 + m];
+                    const uint32_t w0 = __ballot_sync(kFull, hit((m & 1) ? xb[0] : xa[0], z0, dd[0]));
+                    const uint32_t w1 = __ballot_sync(kFull, hit((m & 1) ? xb[1] : xa[1], z0, dd[1]));
+                    if (lane == 0) {
+                        dst0[m] = w0;
+                        dst1[m] = w1;
                     }
-                    if (lane == 0) dst[kSwPlane] = sw;
                 }
             }
             __syncthreads();
 
-            // (3) 4x4 block counts of the batch, per (combo, word): E = even nibbles, O = odd.
-#pragma unroll
-            for (int k = 0; k < kSlots; ++k) {
-                const int p = tid + k * kTpb;
-                if (p < npairs) {
-                    const int combo = p % ncombo, word = p / ncombo;
-                    const int m = combo >> 1;
-                    const uint32_t flip = (uint32_t)((combo ^ m) & 1);  // phase ^ band parity
-                    uint32_t n[4];
-#pragma unroll
-                    for (int q = 0; q < 4; ++q) {
-                        const uint32_t* row = &S.ring[(4 * b + q) % kRing][word][0];
-                        const uint32_t sw = row[kSwPlane];
-                        n[q] = nibble_counts(row[m] & (flip ? sw : ~sw));
-                    }
-                    const uint32_t n01 = n[0] + n[1], n23 = n[2] + n[3];
-                    S.eo_e[combo][word] = (n01 & 0x0F0F0F0Fu) + (n23 & 0x0F0F0F0Fu);
-                    S.eo_o[combo][word] = ((n01 >> 4) & 0x0F0F0F0Fu) + ((n23 >> 4) & 0x0F0F0F0Fu);
+            // ---- survivor queue: flush when half full; groups that did not fit are re-pushed ---
+            if (S.qcount >= kQueueFlush || S.qover)
+                drain_queue(S, a, T, tid, warp, lane, pend, pend_b, false);
+            // Row terms of batch b + 2 (read by the generator after the next barrier).
+            {
+                const int bb = (b + 2) % 3;
+                for (int i = tid; i < 4 * (nb + 1); i += kTpb) {
+                    const int q = i / (nb + 1), e = i % (nb + 1);
+                    const int vi = T.v0 + 4 * (b + 2) + q;
+                    S.rows[bb][q][e] = vi < a.vrows ? a.rt[(int64_t)vi * a.rstride + (e == 0 ? 0 : a.j0 + e)] : 0u;
+                }
+                if (tid < 4) {
+                    const int vi = T.v0 + 4 * (b + 2) + tid;
+                    const int64_t room = a.height_v + 16 - ((int64_t)vi + (int64_t)a.j0 * kPeriod);
+                    uint32_t mask = 0;
+                    if (vi < a.vrows)
+                        for (int m = 0; m < nb; ++m)
+                            if (room - (int64_t)m * kPeriod > 0) mask |= 1u << m;
+                    S.rvalid[bb][tid] = mask;
                 }
             }
-            if (tid == 0) { S.any = 0; S.nsurv = 0; }
-            __syncthreads();
 
-            // (4) 20-column group sums, rolling 20x20 boxes, threshold test.
+            // ---- counter: batch b from ring[buf] ----------------------------------------------
             const int hs = b % 5;
-            uint32_t pend[kSlots];
 #pragma unroll
             for (int k = 0; k < kSlots; ++k) {
-                pend[k] = 0;
-                const int p = tid + k * kTpb;
-                if (p < npairs) {
-                    const int combo = p % ncombo, word = p / ncombo;
-                    const uint32_t e = S.eo_e[combo][word], en = S.eo_e[combo][word + 1];
-                    const uint32_t o = S.eo_o[combo][word], on = S.eo_o[combo][word + 1];
-                    const uint32_t s = e + o, sn = en + on;
-                    const uint32_t s1 = __funnelshift_r(s, sn, 8);
-                    const uint32_t ge = s + s1 + __funnelshift_r(e, en, 16);
-                    const uint32_t go = o + s1 + __funnelshift_r(s, sn, 16);
-                    guard |= ge | go;
-                    re[k] += ge - S.hist_e[hs][p];
-                    ro[k] += go - S.hist_o[hs][p];
-                    S.hist_e[hs][p] = ge;
-                    S.hist_o[hs][p] = go;
-                    if (b >= 4) {
-                        const uint32_t te = (re[k] + bias) & 0x80808080u;
-                        const uint32_t to = (ro[k] + bias) & 0x80808080u;
-                        if (te | to) {
-                            uint32_t gm = group_mask(te, to);
-                            if (word == kWords - 1) gm &= 0x0Fu;  // centres 1,008.. do not exist
-                            pend[k] = gm;
-                            if (gm) S.any = 1;
-                        }
-                    }
-                }
-            }
-            __syncthreads();
-
-            // (5) Exact 221-cell counts of surviving groups, in rounds of kSurvCap groups.
-            if (S.any) {
-                for (;;) {
+                const int combo = warp + kWarps * k;
+                if (combo >= ncombo) break;  // warp-uniform
+                const int m = combo >> 1;
+                uint32_t n[4];
 #pragma unroll
-                    for (int k = 0; k < kSlots; ++k) {
-                        while (pend[k]) {
-                            const int g = __ffs(pend[k]) - 1;
-                            const int idx = atomicAdd(&S.nsurv, 1);
-                            if (idx >= kSurvCap) break;
-                            S.surv[idx] = ((uint32_t)(tid + k * kTpb) << 3) | (uint32_t)g;
-                            pend[k] &= pend[k] - 1;
-                        }
+                for (int q = 0; q < 4; ++q) {
+                    const uint32_t* rec = &S.ring[buf][q][lane][0];
+                    const uint32_t keep = ((S.rvalid[rb][q] >> m) & 1u) ? cm[k] : 0u;
+                    n[q] = nibble_counts(rec[m] & (rec[kSwPlane] ^ fx[k]) & keep);
+                }
+                const uint32_t n01 = n[0] + n[1], n23 = n[2] + n[3];
+                const uint32_t e = (n01 & 0x0F0F0F0Fu) + (n23 & 0x0F0F0F0Fu);
+                const uint32_t o = ((n01 >> 4) & 0x0F0F0F0Fu) + ((n23 >> 4) & 0x0F0F0F0Fu);
+                uint32_t en = __shfl_down_sync(kFull, e, 1), on = __shfl_down_sync(kFull, o, 1);
+                if (lane == kWords - 1) en = on = 0;
+                const uint32_t s = e + o, sn = en + on;
+                const uint32_t s1 = __funnelshift_r(s, sn, 8);
+                const uint32_t ge = s + s1 + __funnelshift_r(e, en, 16);
+                const uint32_t go = o + s1 + __funnelshift_r(s, sn, 16);
+                guard |= (ge + 0x4C4C4C4Cu) | (go + 0x4C4C4C4Cu);
+                re[k] += ge - S.hist_e[hs][combo][lane];
+                ro[k] += go - S.hist_o[hs][combo][lane];
+                S.hist_e[hs][combo][lane] = ge;
+                S.hist_o[hs][combo][lane] = go;
+                // hist_n[hs] held batch b-5; batch b-4 is in slot (b+1)%5.
+                const uint32_t top01 = S.hist_n[(b + 1) % 5][combo][lane];
+                S.hist_n[hs][combo][lane] = n01;
+                uint32_t flag = 0;
+                if (b >= 4) {
+                    const uint32_t te = bytes_at_least(re[k], thr4), to = bytes_at_least(ro[k], thr4);
+                    flag = te | (to >> 1);  // even groups at bits 8k+7, odd at 8k+6
+                    if (lane == kWords - 1) flag &= 0x0000C0C0u;  // groups 4..7: centres >= 1,008
+                }
+                // Second test of flagged groups: drop the 8 outer cells of rows 0, 1 (batch b-4)
+                // and rows 18, 19 (batch b), which no window of the group reaches.
+                const uint32_t top01n = __shfl_down_sync(kFull, top01, 1);
+                const uint32_t n23n = __shfl_down_sync(kFull, n23, 1);
+                if (flag) {
+                    const uint64_t t01 = ((uint64_t)(lane == kWords - 1 ? 0u : top01n) << 32) | top01;
+                    const uint64_t b23 = ((uint64_t)(lane == kWords - 1 ? 0u : n23n) << 32) | n23;
+                    uint32_t gm = 0;
+#pragma unroll
+                    for (int g = 0; g < 8; ++g) {
+                        const int bit = (g & 1) ? 8 * (g >> 1) + 6 : 8 * (g >> 1) + 7;
+                        if (!((flag >> bit) & 1u)) continue;
+                        const uint32_t box = (((g & 1) ? ro[k] : re[k]) >> (8 * (g >> 1))) & 0xFFu;
+                        const uint32_t outer = (uint32_t)((t01 >> (4 * g)) & 0xF) + (uint32_t)((t01 >> (4 * g + 16)) & 0xF) +
+                                               (uint32_t)((b23 >> (4 * g)) & 0xF) + (uint32_t)((b23 >> (4 * g + 16)) & 0xF);
+                        // A box byte of 128+ is a conservative report: keep the group.
+                        if (box >= 128u || box - outer >= (uint32_t)a.min_size) gm |= 1u << g;
                     }
-                    __syncthreads();
-                    const int n = min(S.nsurv, kSurvCap);
-                    for (int i = tid; i < n * 16; i += kTpb) S.cnt[i] = 0;
-                    __syncthreads();
-                    for (int it = tid; it < n * 16 * 17; it += kTpb) {
-                        const int s = it / (16 * 17), rem = it % (16 * 17);
-                        const int d = rem / 17, i = rem % 17;
-                        const uint32_t rec = S.surv[s];
-                        const int p = (int)(rec >> 3), g = (int)(rec & 7);
-                        const int combo = p % ncombo, word = p / ncombo, m = combo >> 1;
-                        const uint32_t flip = (uint32_t)((combo ^ m) & 1);
-                        const int c = word * 32 + 4 * g + (d & 3);
-                        const int rr = 4 * (b - 4) + (d >> 2);
-                        const uint32_t* row = &S.ring[(rr + i) % kRing][0][0];
-                        const int w0 = c >> 5;
-                        const uint32_t sw0 = row[w0 * kPlanes + kSwPlane], sw1 = row[(w0 + 1) * kPlanes + kSwPlane];
-                        const uint32_t lo = row[w0 * kPlanes + m] & (flip ? sw0 : ~sw0);
-                        const uint32_t hi = row[(w0 + 1) * kPlanes + m] & (flip ? sw1 : ~sw1);
-                        const uint32_t bits = __funnelshift_r(lo, hi, c & 31) & window_row_mask(i);
-                        if (bits) atomicAdd(&S.cnt[s * 16 + d], __popc(bits));
-                    }
-                    __syncthreads();
-                    for (int e = tid; e < n * 16; e += kTpb) {
-                        const int s = e >> 4, d = e & 15;
-                        const int count = S.cnt[e];
-                        if (count < a.min_size || (!no_upper && count > a.max_size)) continue;
-                        const uint32_t rec = S.surv[s];
-                        const int p = (int)(rec >> 3), g = (int)(rec & 7);
-                        const int combo = p % ncombo, word = p / ncombo;
-                        const int c = word * 32 + 4 * g + (d & 3);
-                        const int rr = 4 * (b - 4) + (d >> 2);
-                        const int64_t u = (int64_t)u0 + c, v = (int64_t)v0 + rr;
-                        if (c >= kOutW || u >= a.ubase || rr >= out_h) continue;
-                        const int64_t cu = u + (int64_t)(i0 + (combo & 1)) * kPeriod;
-                        const int64_t cv = v + (int64_t)(a.j0 + (combo >> 1)) * kPeriod;
-                        if (cu >= a.width_u || cv >= a.height_v) continue;
-                        const int32_t cx = (int32_t)(a.transposed ? a.area_x0 + cv : a.area_x0 + cu);
-                        const int32_t cz = (int32_t)(a.transposed ? a.area_z0 + cu : a.area_z0 + cv);
-                        if (a.rd_min_sq) {
-                            const int64_t dx = (int64_t)cx - a.center_x, dz = (int64_t)cz - a.center_z;
-                            if (dx * dx + dz * dz < a.rd_min_sq) continue;
-                        }
-                        const unsigned long long idx = atomicAdd(a.emitted, 1ULL);
-                        if (idx < a.cap) a.out[idx] = Hit{count, cx, cz};
-                    }
-                    const int more = __syncthreads_or((pend[0] | pend[1] | pend[2] | pend[3]) != 0);
-                    if (!more) break;
-                    if (tid == 0) S.nsurv = 0;
-                    __syncthreads();
+                    pend[k] = push_groups(S, combo, lane, gm, b);
+                    pend_b[k] = b;
                 }
             }
         }
         __syncthreads();
+        drain_queue(S, a, T, tid, warp, lane, pend, pend_b, true);
     }
-    // A 4-row strip with 32+ hits among 80 cells could carry a box past a byte lane.
-    if (guard & 0xE0E0E0E0u) atomicOr(a.overflow, 1u);
+    // A 4-row strip with 52+ hits among its 80 cells could carry a box past a byte lane.
+    if (guard & 0x80808080u) atomicOr(a.overflow, 1u);
 }
 
 // rt[v * stride + 0] = low 17 bits of the row term of base row v; rt[v * stride + 1 + j] = its
@@ -313,12 +417,18 @@ int band_tile_out_w() { return kOutW; }
 int band_max_bands() { return kMaxBands; }
 
 cudaError_t band_prepare() {
-    return cudaFuncSetAttribute(band_scan_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+    cudaError_t e = cudaFuncSetAttribute(band_scan_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                         (int)sizeof(BandSmem));
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(band_scan_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                 (int)sizeof(BandSmem));
 }
 
 cudaError_t launch_band_scan(const BandArgs& a, int grid, cudaStream_t s) {
-    band_scan_kernel<<<grid, kTpb, sizeof(BandSmem), s>>>(a);
+    if (a.mad_add)
+        band_scan_kernel<true><<<grid, kTpb, sizeof(BandSmem), s>>>(a);
+    else
+        band_scan_kernel<false><<<grid, kTpb, sizeof(BandSmem), s>>>(a);
     return cudaGetLastError();
 }
 

@@ -53,6 +53,7 @@ SIGNATURES = {
     "slime_b200_is_slime_batch": (i32, [i64, vp, vp, u8p, i64]),
     "slime_b200_last_rare_chunks": (i64, []),
     "slime_b200_set_engine": (None, [i32, i32]),
+    "slime_b200_set_tuning": (None, [i32]),
     "slime_b200_microbench": (i32, [i32, i32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
 }
 
