@@ -46,7 +46,8 @@ struct __align__(16) BandSmem {
     uint32_t hist_e[5][kMaxCombos][kWords];   // strip sums of the last 5 batches (even groups)
     uint32_t hist_o[5][kMaxCombos][kWords];   // (odd groups)
     uint32_t hist_n[5][kMaxCombos][kWords];   // nibble counts of rows 0+1 of the last 5 batches
-    uint32_t rows[3][4][kMaxBands + 1];       // row terms of 3 batches: [0] low 17, [1+m] high
+    uint32_t rows[3][4][kMaxBands + 4];       // row terms of 3 batches: [m] high part in band m,
+                                              // [kMaxBands] low 17 bits (16-byte aligned rows)
     uint32_t rvalid[3][4];                    // bit m: the row exists in band m
     uint32_t queue[kQueueCap];                // combo << 24 | word << 19 | group << 16 | batch
     uint32_t scratch[kWarps][20];             // re-evaluation rows, one block per warp
@@ -231,7 +232,8 @@ __global__ void __launch_bounds__(kTpb, 1) band_scan_kernel(const BandArgs a) {
         for (int i = tid; i < 2 * 4 * (nb + 1); i += kTpb) {
             const int bb = i / (4 * (nb + 1)), q = (i / (nb + 1)) % 4, e = i % (nb + 1);
             const int vi = T.v0 + 4 * bb + q;
-            S.rows[bb][q][e] = vi < a.vrows ? a.rt[(int64_t)vi * a.rstride + (e == 0 ? 0 : a.j0 + e)] : 0u;
+            S.rows[bb][q][e == 0 ? kMaxBands : e - 1] =
+                vi < a.vrows ? a.rt[(int64_t)vi * a.rstride + (e == 0 ? 0 : a.j0 + e)] : 0u;
         }
         if (tid < 8) {
             const int bb = tid >> 2, q = tid & 3, vi = T.v0 + 4 * bb + q;
@@ -250,8 +252,8 @@ __global__ void __launch_bounds__(kTpb, 1) band_scan_kernel(const BandArgs a) {
 #pragma unroll 1
             for (int q = 0; q < 4; ++q) {
                 const uint32_t* zr = &S.rows[rb][q][0];
-                const uint32_t zlo = zr[0];
-                const uint32_t zpar = (zr[1] ^ kXorHi) & 1u;
+                const uint32_t zlo = zr[kMaxBands];
+                const uint32_t zpar = (zr[0] ^ kXorHi) & 1u;
                 uint32_t xa[2], xb[2], dd[2];
 #pragma unroll
                 for (int k = 0; k < 2; ++k) {
@@ -271,7 +273,8 @@ __global__ void __launch_bounds__(kTpb, 1) band_scan_kernel(const BandArgs a) {
                 };
                 int m = 0;
                 for (; m + 3 < nb; m += 4) {
-                    const uint32_t z0 = zr[1 + m], z1 = zr[2 + m], z2 = zr[3 + m], z3 = zr[4 + m];
+                    const uint4 z4 = *reinterpret_cast<const uint4*>(zr + m);  // m % 4 == 0: aligned
+                    const uint32_t z0 = z4.x, z1 = z4.y, z2 = z4.z, z3 = z4.w;
                     const uint32_t a0 = __ballot_sync(kFull, hit(xa[0], z0, dd[0]));
                     const uint32_t a1 = __ballot_sync(kFull, hit(xa[1], z0, dd[1]));
                     const uint32_t b0 = __ballot_sync(kFull, hit(xb[0], z1, dd[0]));
@@ -286,7 +289,7 @@ __global__ void __launch_bounds__(kTpb, 1) band_scan_kernel(const BandArgs a) {
                     }
                 }
                 for (; m < nb; ++m) {
-                    const uint32_t z0 = zr[1 + m];
+                    const uint32_t z0 = zr[m];
                     const uint32_t w0 = __ballot_sync(kFull, hit((m & 1) ? xb[0] : xa[0], z0, dd[0]));
                     const uint32_t w1 = __ballot_sync(kFull, hit((m & 1) ? xb[1] : xa[1], z0, dd[1]));
                     if (lane == 0) {
@@ -306,7 +309,8 @@ __global__ void __launch_bounds__(kTpb, 1) band_scan_kernel(const BandArgs a) {
                 for (int i = tid; i < 4 * (nb + 1); i += kTpb) {
                     const int q = i / (nb + 1), e = i % (nb + 1);
                     const int vi = T.v0 + 4 * (b + 2) + q;
-                    S.rows[bb][q][e] = vi < a.vrows ? a.rt[(int64_t)vi * a.rstride + (e == 0 ? 0 : a.j0 + e)] : 0u;
+                    S.rows[bb][q][e == 0 ? kMaxBands : e - 1] =
+                        vi < a.vrows ? a.rt[(int64_t)vi * a.rstride + (e == 0 ? 0 : a.j0 + e)] : 0u;
                 }
                 if (tid < 4) {
                     const int vi = T.v0 + 4 * (b + 2) + tid;
