@@ -54,11 +54,13 @@ bool Context::scan_band(const SearchSpec& q, std::vector<Hit>& best, std::vector
     const int64_t nI = (width_u + kP - 1) / kP, nJ = (height_v + kP - 1) / kP;
     const int32_t ubase = (int32_t)std::min(kP, width_u), vbase = (int32_t)std::min(kP, height_v);
     const int32_t vrows = vbase + 16;
-    const int32_t rstride = (int32_t)(1 + nJ);
+    const int32_t vrows_alloc = vbase + 32;  // zero rows: 8-row bulk copies never run past the end
+    const int nb_max = band_max_bands();
+    const int64_t ngroups = (nJ + nb_max - 1) / nb_max;
     const int out_w = band_tile_out_w();
     cudaError_t e;
     if ((e = xt.reserve((size_t)width_u + 16)) != cudaSuccess ||
-        (e = rt.reserve((size_t)vrows * rstride)) != cudaSuccess ||
+        (e = rt.reserve((size_t)ngroups * vrows_alloc * band_row_words())) != cudaSuccess ||
         (e = counters.reserve(4)) != cudaSuccess ||
         (e = hits.reserve(hit_capacity(q.max_results))) != cudaSuccess ||
         (e = fixed.reserve(1u << 20)) != cudaSuccess) {
@@ -67,7 +69,7 @@ bool Context::scan_band(const SearchSpec& q, std::vector<Hit>& best, std::vector
     }
     const int32_t col_first = (transposed ? area_z0 : area_x0) - 8;
     const int32_t row_first = (transposed ? area_x0 : area_z0) - 8;
-    if ((e = launch_band_terms(xt.ptr, col_first, (int32_t)(width_u + 16), rt.ptr, rstride, vrows,
+    if ((e = launch_band_terms(xt.ptr, col_first, (int32_t)(width_u + 16), rt.ptr, vrows_alloc, vrows,
                                (int32_t)nJ, row_first, height_v + 16, q.seed, transposed, stream)) != cudaSuccess) {
         set_error("band terms", e);
         return false;
@@ -89,8 +91,6 @@ bool Context::scan_band(const SearchSpec& q, std::vector<Hit>& best, std::vector
     if (nrare > kRareCap) { set_error("too many rare chunks", cudaErrorMemoryAllocation); return false; }
     last_rare = nrare;
 
-    const int nb_max = band_max_bands();
-    const int64_t ngroups = (nJ + nb_max - 1) / nb_max;
     const int32_t band_h = (int32_t)std::min<int64_t>(2048, std::max<int64_t>(256, vbase));
     const int64_t u_tiles = (ubase + out_w - 1) / out_w, v_tiles = (vbase + band_h - 1) / band_h;
     const int64_t pairs = (nI + 1) / 2;
@@ -98,9 +98,8 @@ bool Context::scan_band(const SearchSpec& q, std::vector<Hit>& best, std::vector
     const uint64_t cap = hits.count;
 
     for (int64_t g = 0; g < ngroups; ++g) {
-        const int32_t per = (int32_t)((nJ + ngroups - 1) / ngroups);
-        const int32_t j0 = (int32_t)(g * per);
-        const int32_t nb = (int32_t)std::min<int64_t>(per, nJ - j0);
+        const int32_t j0 = (int32_t)(g * nb_max);
+        const int32_t nb = (int32_t)std::min<int64_t>(nb_max, nJ - j0);
         if (nb <= 0) break;
         const int64_t tiles = u_tiles * v_tiles * pairs;
         int64_t chunk = std::max<int64_t>(grid, std::min<int64_t>(tiles, (int64_t)grid * 24));
@@ -111,8 +110,7 @@ bool Context::scan_band(const SearchSpec& q, std::vector<Hit>& best, std::vector
             BandArgs a{};
             a.ct = xt.ptr;
             a.ncols = width_u + 16;
-            a.rt = rt.ptr;
-            a.rstride = rstride;
+            a.rt = rt.ptr + (size_t)g * vrows_alloc * band_row_words();
             a.vrows = vrows;
             a.vbase = vbase;
             a.ubase = ubase;
@@ -238,6 +236,7 @@ bool Context::scan_band(const SearchSpec& q, std::vector<Hit>& best, std::vector
         set_error("flags", e);
         return false;
     }
+    if (*(uint32_t*)pinned & 4u) { set_error("band engine: row-term copy timed out", cudaErrorLaunchTimeout); return false; }
     if (*(uint32_t*)pinned) {
         // A 4-row strip too dense for the byte-lane box: redo the search with the general scan.
         band_fallbacks++;

@@ -68,8 +68,7 @@ cudaError_t launch_predicate(int64_t seed, const int64_t* x, const int64_t* z, u
 struct BandArgs {
     const uint64_t* ct;      // column terms (phase axis, no seed), ncols = width_u + 16 entries
     int64_t ncols;
-    const uint32_t* rt;      // packed row terms (see row_terms_kernel), vrows x rstride
-    int32_t rstride;
+    const uint32_t* rt;      // row-term records of this band group (see row_terms_kernel)
     int32_t vrows;           // base input rows = vbase + 16
     int32_t vbase;           // base centre rows = min(2^17, height_v)
     int32_t ubase;           // base centre columns owned = min(2^17, width_u)
@@ -95,8 +94,9 @@ int band_tile_out_w();
 int band_max_bands();
 cudaError_t band_prepare();
 cudaError_t launch_band_scan(const BandArgs& a, int grid, cudaStream_t s);
+int band_row_words();
 cudaError_t launch_band_terms(uint64_t* ct, int32_t col_first, int32_t ncols, uint32_t* rt,
-                              int32_t rstride, int32_t vrows, int32_t nj, int32_t row_first,
+                              int32_t vrows_alloc, int32_t vrows, int32_t nj, int32_t row_first,
                               int64_t row_limit, int64_t seed, bool transposed, cudaStream_t s);
 
 // ---- rare redraw correction (rare_fix.cu) ------------------------------------------------

@@ -9,8 +9,9 @@
 //    position the low-17-bit work (carry, Q, D, parity) is done once; per band it costs one add,
 //    one xor, one multiply-add, one compare and one ballot for the two phases together, because
 //    the parity tells which of the two phases can be a first-draw slime chunk.
-//  * Rows advance in batches of 4. Ballots of a batch go to one of two 4-row buffers, so one
-//    barrier per batch separates the generator (batch b+1) from the counter (batch b).
+//  * Rows advance in batches of 8 (two 4-row strips). Ballots of a batch go to one of two
+//    buffers, so one barrier per batch separates the generator (batch b+1) from the counter
+//    (batch b). Row terms arrive by TMA bulk copies two batches ahead.
 //  * Counting is SWAR in byte lanes on 4x4 centre groups. A warp owns a combo (phase, band) row
 //    with one lane per 32-column word: nibble popcounts of the 4 rows give 4x4 block counts,
 //    the neighbour word comes by shuffle, three funnel shifts and two adds give the 20-column
@@ -34,30 +35,67 @@ constexpr int kWords = 32;                  // words per ring row: 1,024 base co
 constexpr int kOutW = kWords * 32 - 16;     // 1,008 centres per tile row
 constexpr int kMaxBands = 32;
 constexpr int kSwPlane = kMaxBands;         // plane of the phase-swap ballot
-constexpr int kPlanes = kMaxBands + 4;      // 16-byte aligned word records
+constexpr int kPlanes = kMaxBands + 1;      // band planes and the swap plane
 constexpr int kMaxCombos = 2 * kMaxBands;
 constexpr int kSlots = kMaxCombos / kWarps; // combo rows counted per warp
 constexpr int kQueueCap = 1024;
 constexpr int kQueueFlush = 512;
 constexpr unsigned kFull = 0xFFFFFFFFu;
 
+// Row-term record of one base row for one group of up to 32 bands (matches the global table
+// written by row_terms_kernel, so a batch of 4 rows is one contiguous 576-byte bulk copy).
+constexpr int kRowWords = 36;
+constexpr int kRowLo = 32;      // low 17 bits of the row term (shared by all bands)
+constexpr int kRowValid = 33;   // bands of the group that hold this row (prefix count)
+
+constexpr int kBatchRows = 8;               // rows per barrier: two 4-row strips
+
 struct __align__(16) BandSmem {
-    uint32_t ring[2][4][kWords][kPlanes];     // [buffer][row][word][band planes | swap plane]
-    uint32_t hist_e[5][kMaxCombos][kWords];   // strip sums of the last 5 batches (even groups)
+    uint32_t ring[2][kBatchRows][kPlanes][kWords];  // [buffer][row][band planes | swap][word]
+    uint32_t hist_e[5][kMaxCombos][kWords];   // strip sums of the last 5 strips (even groups)
     uint32_t hist_o[5][kMaxCombos][kWords];   // (odd groups)
-    uint32_t hist_n[5][kMaxCombos][kWords];   // nibble counts of rows 0+1 of the last 5 batches
-    uint32_t rows[3][4][kMaxBands + 4];       // row terms of 3 batches: [m] high part in band m,
-                                              // [kMaxBands] low 17 bits (16-byte aligned rows)
-    uint32_t rvalid[3][4];                    // bit m: the row exists in band m
-    uint32_t queue[kQueueCap];                // combo << 24 | word << 19 | group << 16 | batch
+    uint32_t hist_n[5][kMaxCombos][kWords];   // nibble counts of rows 0+1 of the last 5 strips
+    uint32_t rows[3][kBatchRows][kRowWords];  // row terms of 3 batches, filled by bulk copies
+    unsigned long long rows_bar[3];           // mbarriers of the three row-term buffers
+    uint32_t queue[kQueueCap];                // combo << 24 | word << 19 | group << 16 | strip
     uint32_t scratch[kWarps][20];             // re-evaluation rows, one block per warp
     int qcount;
     int qover;
+    int failed;  // a bounded wait gave up: the CTA stops
 };
 
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return (uint32_t)__cvta_generic_to_shared(p);
+}
+
+// Bulk copy (TMA engine, no multicast) of `bytes` from global memory into shared memory,
+// completing on an mbarrier. Addresses and size are multiples of 16 bytes.
+__device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t bytes,
+                                          unsigned long long* bar) {
+    asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
+                 :: "r"(smem_u32(bar)), "r"(bytes) : "memory");
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];"
+                 :: "r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
+}
+
+// Waits for the mbarrier phase with the given parity; gives up after a bounded number of polls
+// and returns false (the caller flags an error instead of hanging the GPU).
+__device__ __forceinline__ bool bar_wait(unsigned long long* bar, uint32_t parity) {
+    for (int i = 0; i < (1 << 22); ++i) {
+        uint32_t done;
+        asm volatile("{ .reg .pred p;\n"
+                     "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
+                     "selp.u32 %0, 1, 0, p; }"
+                     : "=r"(done) : "r"(smem_u32(bar)), "r"(parity) : "memory");
+        if (done) return true;
+    }
+    return false;
+}
+
 __device__ __forceinline__ uint32_t nibble_counts(uint32_t r) {
-    const uint32_t a = r - ((r >> 1) & 0x55555555u);
-    return (a & 0x33333333u) + ((a >> 2) & 0x33333333u);
+    const uint32_t a = r - (__umulhi(r, 1u << 31) & 0x55555555u);
+    return (a & 0x33333333u) + (__umulhi(a, 1u << 30) & 0x33333333u);
 }
 
 // Per byte: high bit set where v >= t (v, t < 256; borrow-free because v | 0x80 >= 128 >= t').
@@ -92,10 +130,10 @@ __device__ void flush_queue(BandSmem& S, const BandArgs& a, const Tile& T, int w
     for (int s = warp; s < n; s += kWarps) {
         const uint32_t rec = S.queue[s];
         const int combo = (int)(rec >> 24), word = (int)((rec >> 19) & 31);
-        const int g = (int)((rec >> 16) & 7), b = (int)(rec & 0xFFFF);
+        const int g = (int)((rec >> 16) & 7), st = (int)(rec & 0xFFFF);
         const int ph = combo & 1, m = combo >> 1;
         const int c0 = word * 32 + 4 * g;       // first window column (tile-relative input col)
-        const int r0 = 4 * (b - 4);             // first window row (tile-relative input row)
+        const int r0 = 4 * (st - 4);            // first window row (tile-relative input row)
         uint64_t xt = 0;
         if (lane < 20) {
             const int64_t idx = (int64_t)T.u0 + c0 + lane + (int64_t)(T.i0 + ph) * kPeriod;
@@ -105,8 +143,8 @@ __device__ void flush_queue(BandSmem& S, const BandArgs& a, const Tile& T, int w
             const int vi = T.v0 + r0 + t;
             uint64_t zt = 0;
             if (vi < a.vrows) {
-                const uint32_t* row = a.rt + (int64_t)vi * a.rstride;
-                zt = (uint64_t)row[0] | ((uint64_t)row[1 + a.j0 + m] << kPeriodBits);
+                const uint32_t* row = a.rt + (int64_t)vi * kRowWords;
+                zt = (uint64_t)row[kRowLo] | ((uint64_t)row[m] << kPeriodBits);
             }
             const uint32_t bits = __ballot_sync(kFull, lane < 20 && first_draw_slime(xt, zt));
             if (lane == 0) S.scratch[warp][t] = bits;
@@ -148,11 +186,102 @@ __device__ void flush_queue(BandSmem& S, const BandArgs& a, const Tile& T, int w
     }
 }
 
+// Per-thread counter state: one entry per combo slot of the warp (lane = word).
+struct Counter {
+    uint32_t cm[kSlots];      // columns of the word that exist for the slot's phase
+    uint32_t fx[kSlots];      // ~0 where the swap ballot is inverted to select the combo's phase
+    uint32_t re[kSlots], ro[kSlots];  // rolling 20x20 boxes (even / odd groups, byte lanes)
+    uint32_t pend[kSlots][2]; // flagged groups that did not fit in the queue, per strip of the
+    int pend_s[kSlots][2];    // batch (all are re-pushed before the next batch is counted)
+};
+
+// Counts one 4-row strip (rows r0..r0+3 of ring[buf]) for every combo slot of this warp:
+// 4x4 block counts, 20-column strip sums, rolling 20x20 boxes, threshold test, the trimmed
+// second test of flagged groups, and queueing of the survivors.
+template <bool kMasked>
+__device__ __forceinline__ void count_strip(BandSmem& S, const BandArgs& a, Counter& C, int buf,
+                                            int rb, int t, int st, int warp, int lane, int ncombo,
+                                            uint32_t thr4, uint32_t& guard) {
+    const int r0 = 4 * t;  // t is a compile-time constant after unrolling: static register indexing
+    const int hs = st % 5;
+    uint32_t rvalid[4];
+    if (kMasked) {
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const uint32_t nv = S.rows[rb][r0 + q][kRowValid];
+            rvalid[q] = nv >= 32 ? ~0u : (1u << nv) - 1u;
+        }
+    }
+#pragma unroll
+    for (int k = 0; k < kSlots; ++k) {
+        const int combo = warp + kWarps * k;
+        if (combo < ncombo) {  // warp-uniform
+            const int m = combo >> 1;
+            uint32_t n[4];
+#pragma unroll
+            for (int q = 0; q < 4; ++q) {
+                uint32_t w = S.ring[buf][r0 + q][m][lane] & (S.ring[buf][r0 + q][kSwPlane][lane] ^ C.fx[k]);
+                if (kMasked) w &= ((rvalid[q] >> m) & 1u) ? C.cm[k] : 0u;
+                n[q] = nibble_counts(w);
+            }
+            const uint32_t n01 = n[0] + n[1], n23 = n[2] + n[3];
+            const uint32_t e = (n01 & 0x0F0F0F0Fu) + (n23 & 0x0F0F0F0Fu);
+            const uint32_t o = ((n01 >> 4) & 0x0F0F0F0Fu) + ((n23 >> 4) & 0x0F0F0F0Fu);
+            uint32_t en = __shfl_down_sync(kFull, e, 1), on = __shfl_down_sync(kFull, o, 1);
+            if (lane == kWords - 1) en = on = 0;
+            const uint32_t s = e + o, sn = en + on;
+            const uint32_t s1 = __funnelshift_r(s, sn, 8);
+            const uint32_t ge = s + s1 + __funnelshift_r(e, en, 16);
+            const uint32_t go = o + s1 + __funnelshift_r(s, sn, 16);
+            guard |= (ge + 0x4C4C4C4Cu) | (go + 0x4C4C4C4Cu);
+            uint32_t* he = &S.hist_e[hs][combo][lane];
+            uint32_t* ho = &S.hist_o[hs][combo][lane];
+            C.re[k] += ge - *he;
+            C.ro[k] += go - *ho;
+            *he = ge;
+            *ho = go;
+            S.hist_n[hs][combo][lane] = n01;
+            uint32_t flag = 0;
+            if (st >= 4) {
+                const uint32_t te = bytes_at_least(C.re[k], thr4), to = bytes_at_least(C.ro[k], thr4);
+                flag = te | (to >> 1);  // even groups at bits 8k+7, odd at 8k+6
+                if (lane == kWords - 1) flag &= 0x0000C0C0u;  // groups 4..7: centres >= 1,008
+            }
+            // Second test of flagged groups: drop the 8 outer cells of rows 0, 1 (strip st-4) and
+            // rows 18, 19 (strip st), which no window of the group reaches.
+            if (__any_sync(kFull, flag != 0)) {
+                const uint32_t top01 = S.hist_n[(st + 1) % 5][combo][lane];  // strip st - 4
+                const uint32_t top01n = __shfl_down_sync(kFull, top01, 1);
+                const uint32_t n23n = __shfl_down_sync(kFull, n23, 1);
+                if (flag) {
+                    const uint64_t t01 = ((uint64_t)(lane == kWords - 1 ? 0u : top01n) << 32) | top01;
+                    const uint64_t b23 = ((uint64_t)(lane == kWords - 1 ? 0u : n23n) << 32) | n23;
+                    uint32_t gm = 0;
+#pragma unroll
+                    for (int g = 0; g < 8; ++g) {
+                        const int bit = (g & 1) ? 8 * (g >> 1) + 6 : 8 * (g >> 1) + 7;
+                        if (!((flag >> bit) & 1u)) continue;
+                        const uint32_t box = (((g & 1) ? C.ro[k] : C.re[k]) >> (8 * (g >> 1))) & 0xFFu;
+                        const uint32_t outer = (uint32_t)((t01 >> (4 * g)) & 0xF) + (uint32_t)((t01 >> (4 * g + 16)) & 0xF) +
+                                               (uint32_t)((b23 >> (4 * g)) & 0xF) + (uint32_t)((b23 >> (4 * g + 16)) & 0xF);
+                        // A box byte of 128+ is a conservative report: keep the group.
+                        if (box >= 128u || box - outer >= (uint32_t)a.min_size) gm |= 1u << g;
+                    }
+                    if (gm) {
+                        C.pend[k][t] = push_groups(S, combo, lane, gm, st);
+                        C.pend_s[k][t] = st;
+                    }
+                }
+            }
+        }
+    }
+}
+
 // Processes the queue (all threads; block-uniform entry) and re-pushes pending groups. With
 // `final` it repeats until queue and pending groups are empty; otherwise it may return with a
 // partial queue (fewer than kQueueFlush groups) and no pending groups.
-__device__ void drain_queue(BandSmem& S, const BandArgs& a, const Tile& T, int tid, int warp,
-                            int lane, uint32_t (&pend)[kSlots], int (&pend_b)[kSlots], bool final) {
+__device__ __forceinline__ void drain_queue(BandSmem& S, const BandArgs& a, const Tile& T, int tid, int warp,
+                            int lane, Counter& C, bool final) {
     for (;;) {
         flush_queue(S, a, T, warp, lane);
         __syncthreads();
@@ -161,8 +290,11 @@ __device__ void drain_queue(BandSmem& S, const BandArgs& a, const Tile& T, int t
         bool left = false;
 #pragma unroll
         for (int k = 0; k < kSlots; ++k) {
-            if (pend[k]) pend[k] = push_groups(S, warp + kWarps * k, lane, pend[k], pend_b[k]);
-            left |= pend[k] != 0;
+#pragma unroll
+            for (int t = 0; t < 2; ++t) {
+                if (C.pend[k][t]) C.pend[k][t] = push_groups(S, warp + kWarps * k, lane, C.pend[k][t], C.pend_s[k][t]);
+                left |= C.pend[k][t] != 0;
+            }
         }
         const bool more = __syncthreads_or(left);
         const int queued = S.qcount;  // stable: every push precedes the barrier above
@@ -180,7 +312,16 @@ __global__ void __launch_bounds__(kTpb, 1) band_scan_kernel(const BandArgs a) {
     const uint32_t thr4 = (uint32_t)min(a.min_size, 128) * 0x01010101u;
     const uint32_t one = a.one;  // 1 at run time: keeps the band add on the multiply pipe
     uint32_t guard = 0;
-    if (tid == 0) { S.qcount = 0; S.qover = 0; }
+    uint32_t bar_phase = 0;  // bit r: parity of the next completion of rows_bar[r]
+    if (tid == 0) {
+        S.qcount = 0;
+        S.qover = 0;
+        S.failed = 0;
+        for (int r = 0; r < 3; ++r)
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&S.rows_bar[r])) : "memory");
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
 
     for (int64_t tile = a.tile_begin + blockIdx.x; tile < a.tile_end; tile += gridDim.x) {
         Tile T;
@@ -195,13 +336,17 @@ __global__ void __launch_bounds__(kTpb, 1) band_scan_kernel(const BandArgs a) {
             (int64_t)T.v0 + (int64_t)a.j0 * kPeriod >= a.height_v)
             continue;
         T.out_h = min(a.band_h, a.vbase - T.v0);
-        const int batches = (T.out_h + 16 + 3) / 4;
+        const int strips = (T.out_h + 16 + 3) / 4;
+        const int batches = (strips + 1) / 2;
+        constexpr uint32_t kBatchBytes = kBatchRows * kRowWords * 4;
 
-        // Generator columns of this thread: words 2*warp and 2*warp+1, lane = bit.
-        uint32_t lox[2], xh0[2], xh1[2];
+        // Generator columns of this thread: words 4*(warp%8) .. +3, lane = bit; the warp
+        // generates rows 4*(warp/8) .. +3 of every 8-row batch.
+        const int gw = (warp & 7) * 4, gq = (warp >> 3) * 4;
+        uint32_t lox[4], xh0[4], xh1[4];
 #pragma unroll
-        for (int k = 0; k < 2; ++k) {
-            const int64_t idx0 = (int64_t)T.u0 + (warp * 2 + k) * 32 + lane + (int64_t)T.i0 * kPeriod;
+        for (int k = 0; k < 4; ++k) {
+            const int64_t idx0 = (int64_t)T.u0 + (gw + k) * 32 + lane + (int64_t)T.i0 * kPeriod;
             const uint64_t x0 = idx0 < a.ncols ? a.ct[idx0] : 0;
             const uint64_t x1 = idx0 + kPeriod < a.ncols ? a.ct[idx0 + kPeriod] : 0;
             lox[k] = (uint32_t)x0 & 0x1FFFFu;
@@ -210,201 +355,146 @@ __global__ void __launch_bounds__(kTpb, 1) band_scan_kernel(const BandArgs a) {
         }
         // Counter slots of this warp: combo rows warp + 16*k; lane = word. Columns of the word
         // that exist for the slot's phase (bits beyond are masked to zero before counting).
-        uint32_t cm[kSlots], fx[kSlots], re[kSlots], ro[kSlots], pend[kSlots];
-        int pend_b[kSlots];
+        Counter C;
 #pragma unroll
         for (int k = 0; k < kSlots; ++k) {
             const int combo = warp + kWarps * k;
             const int64_t first = (int64_t)T.u0 + lane * 32 + (int64_t)(T.i0 + (combo & 1)) * kPeriod;
             const int64_t nvalid = a.ncols - first;
-            cm[k] = nvalid >= 32 ? ~0u : nvalid <= 0 ? 0u : (1u << nvalid) - 1u;
-            fx[k] = ((combo ^ (combo >> 1)) & 1) ? 0u : ~0u;
-            re[k] = ro[k] = 0;
-            pend[k] = 0;
-            pend_b[k] = 0;
+            C.cm[k] = nvalid >= 32 ? ~0u : nvalid <= 0 ? 0u : (1u << nvalid) - 1u;
+            C.fx[k] = ((combo ^ (combo >> 1)) & 1) ? 0u : ~0u;
+            C.re[k] = C.ro[k] = 0;
+            C.pend[k][0] = C.pend[k][1] = 0;
+            C.pend_s[k][0] = C.pend_s[k][1] = 0;
         }
+        // Interior tiles (every column of both phases and every row of every band exists) skip
+        // the validity masks (block-uniform).
+        const bool interior =
+            (int64_t)T.u0 + kWords * 32 + (int64_t)(T.i0 + 1) * kPeriod <= a.ncols &&
+            (int64_t)T.v0 + (int64_t)batches * kBatchRows + (int64_t)(a.j0 + nb - 1) * kPeriod <= a.height_v + 16 &&
+            T.v0 + batches * kBatchRows <= a.vrows;
         for (int i = tid; i < 5 * kMaxCombos * kWords; i += kTpb) {
             (&S.hist_e[0][0][0])[i] = 0;
             (&S.hist_o[0][0][0])[i] = 0;
             (&S.hist_n[0][0][0])[i] = 0;
         }
-        // Row terms of batches 0 and 1.
-        for (int i = tid; i < 2 * 4 * (nb + 1); i += kTpb) {
-            const int bb = i / (4 * (nb + 1)), q = (i / (nb + 1)) % 4, e = i % (nb + 1);
-            const int vi = T.v0 + 4 * bb + q;
-            S.rows[bb][q][e == 0 ? kMaxBands : e - 1] =
-                vi < a.vrows ? a.rt[(int64_t)vi * a.rstride + (e == 0 ? 0 : a.j0 + e)] : 0u;
-        }
-        if (tid < 8) {
-            const int bb = tid >> 2, q = tid & 3, vi = T.v0 + 4 * bb + q;
-            const int64_t room = a.height_v + 16 - ((int64_t)vi + (int64_t)a.j0 * kPeriod);
-            uint32_t mask = 0;
-            if (vi < a.vrows)
-                for (int m = 0; m < nb; ++m)
-                    if (room - (int64_t)m * kPeriod > 0) mask |= 1u << m;
-            S.rvalid[bb][q] = mask;
+        // Row terms of batches 0 and 1 (batch b lives in rows[b % 3]).
+        if (tid == 0) {
+            bulk_load(&S.rows[0][0][0], a.rt + (int64_t)T.v0 * kRowWords, kBatchBytes, &S.rows_bar[0]);
+            if (batches > 1)
+                bulk_load(&S.rows[1][0][0], a.rt + (int64_t)(T.v0 + kBatchRows) * kRowWords, kBatchBytes, &S.rows_bar[1]);
         }
         __syncthreads();
 
         for (int b = 0; b < batches; ++b) {
             const int rb = b % 3, buf = b & 1;
             // ---- generator: batch b into ring[buf] ------------------------------------------
+            if (!bar_wait(&S.rows_bar[rb], (bar_phase >> rb) & 1u)) {
+                S.failed = 1;
+                if (lane == 0) atomicOr(a.overflow, 4u);
+            }
+            bar_phase ^= 1u << rb;
 #pragma unroll 1
-            for (int q = 0; q < 4; ++q) {
+            for (int qq = 0; qq < 4; ++qq) {
+                const int q = gq + qq;
                 const uint32_t* zr = &S.rows[rb][q][0];
-                const uint32_t zlo = zr[kMaxBands];
+                const uint32_t zlo = zr[kRowLo];
                 const uint32_t zpar = (zr[0] ^ kXorHi) & 1u;
-                uint32_t xa[2], xb[2], dd[2];
+                uint32_t xa[4], xb[4], dd[4], sw[4];
 #pragma unroll
-                for (int k = 0; k < 2; ++k) {
+                for (int k = 0; k < 4; ++k) {
                     const Shared sh = shared_part(lox[k], zlo);
                     const uint32_t pi = (sh.q0 ^ xh0[k] ^ sh.carry ^ zpar) & 1u;
                     xa[k] = (pi ? xh1[k] : xh0[k]) + sh.carry;
                     xb[k] = (pi ? xh0[k] : xh1[k]) + sh.carry;
                     dd[k] = sh.d;
-                    const uint32_t sw = __ballot_sync(kFull, pi != 0);
-                    if (lane == 0) S.ring[buf][q][warp * 2 + k][kSwPlane] = sw;
+                    sw[k] = __ballot_sync(kFull, pi != 0);
                 }
-                uint32_t* dst0 = &S.ring[buf][q][warp * 2][0];
-                uint32_t* dst1 = &S.ring[buf][q][warp * 2 + 1][0];
+                uint32_t* dst = &S.ring[buf][q][0][gw];  // plane m at dst + m * kWords, 16-byte aligned
+                if (lane == 0) *reinterpret_cast<uint4*>(dst + kSwPlane * kWords) = make_uint4(sw[0], sw[1], sw[2], sw[3]);
                 auto hit = [&](uint32_t x, uint32_t z, uint32_t d) {
                     const uint32_t t = kMadAdd ? z * one + x : z + x;
                     return ((t ^ kXorHi) * kMulH + d) < kHitBelow;
                 };
                 int m = 0;
-                for (; m + 3 < nb; m += 4) {
-                    const uint4 z4 = *reinterpret_cast<const uint4*>(zr + m);  // m % 4 == 0: aligned
-                    const uint32_t z0 = z4.x, z1 = z4.y, z2 = z4.z, z3 = z4.w;
-                    const uint32_t a0 = __ballot_sync(kFull, hit(xa[0], z0, dd[0]));
-                    const uint32_t a1 = __ballot_sync(kFull, hit(xa[1], z0, dd[1]));
-                    const uint32_t b0 = __ballot_sync(kFull, hit(xb[0], z1, dd[0]));
-                    const uint32_t b1 = __ballot_sync(kFull, hit(xb[1], z1, dd[1]));
-                    const uint32_t c0 = __ballot_sync(kFull, hit(xa[0], z2, dd[0]));
-                    const uint32_t c1 = __ballot_sync(kFull, hit(xa[1], z2, dd[1]));
-                    const uint32_t e0 = __ballot_sync(kFull, hit(xb[0], z3, dd[0]));
-                    const uint32_t e1 = __ballot_sync(kFull, hit(xb[1], z3, dd[1]));
+                for (; m + 1 < nb; m += 2) {
+                    const uint2 z2 = *reinterpret_cast<const uint2*>(zr + m);  // m even: aligned
+                    uint32_t wa[4], wb[4];
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        wa[k] = __ballot_sync(kFull, hit(xa[k], z2.x, dd[k]));
+                        wb[k] = __ballot_sync(kFull, hit(xb[k], z2.y, dd[k]));
+                    }
                     if (lane == 0) {
-                        *reinterpret_cast<uint4*>(dst0 + m) = make_uint4(a0, b0, c0, e0);
-                        *reinterpret_cast<uint4*>(dst1 + m) = make_uint4(a1, b1, c1, e1);
+                        *reinterpret_cast<uint4*>(dst + m * kWords) = make_uint4(wa[0], wa[1], wa[2], wa[3]);
+                        *reinterpret_cast<uint4*>(dst + (m + 1) * kWords) = make_uint4(wb[0], wb[1], wb[2], wb[3]);
                     }
                 }
-                for (; m < nb; ++m) {
+                if (m < nb) {  // odd band count: the last band uses the even-band phase choice
                     const uint32_t z0 = zr[m];
-                    const uint32_t w0 = __ballot_sync(kFull, hit((m & 1) ? xb[0] : xa[0], z0, dd[0]));
-                    const uint32_t w1 = __ballot_sync(kFull, hit((m & 1) ? xb[1] : xa[1], z0, dd[1]));
-                    if (lane == 0) {
-                        dst0[m] = w0;
-                        dst1[m] = w1;
-                    }
+                    uint32_t wa[4];
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) wa[k] = __ballot_sync(kFull, hit(xa[k], z0, dd[k]));
+                    if (lane == 0) *reinterpret_cast<uint4*>(dst + m * kWords) = make_uint4(wa[0], wa[1], wa[2], wa[3]);
                 }
             }
             __syncthreads();
+            if (S.failed) return;  // block-uniform after the barrier
 
             // ---- survivor queue: flush when half full; groups that did not fit are re-pushed ---
             if (S.qcount >= kQueueFlush || S.qover)
-                drain_queue(S, a, T, tid, warp, lane, pend, pend_b, false);
-            // Row terms of batch b + 2 (read by the generator after the next barrier).
-            {
-                const int bb = (b + 2) % 3;
-                for (int i = tid; i < 4 * (nb + 1); i += kTpb) {
-                    const int q = i / (nb + 1), e = i % (nb + 1);
-                    const int vi = T.v0 + 4 * (b + 2) + q;
-                    S.rows[bb][q][e == 0 ? kMaxBands : e - 1] =
-                        vi < a.vrows ? a.rt[(int64_t)vi * a.rstride + (e == 0 ? 0 : a.j0 + e)] : 0u;
-                }
-                if (tid < 4) {
-                    const int vi = T.v0 + 4 * (b + 2) + tid;
-                    const int64_t room = a.height_v + 16 - ((int64_t)vi + (int64_t)a.j0 * kPeriod);
-                    uint32_t mask = 0;
-                    if (vi < a.vrows)
-                        for (int m = 0; m < nb; ++m)
-                            if (room - (int64_t)m * kPeriod > 0) mask |= 1u << m;
-                    S.rvalid[bb][tid] = mask;
-                }
-            }
+                drain_queue(S, a, T, tid, warp, lane, C, false);
+            // Row terms of batch b + 2 (its buffer was last read before this batch's barrier).
+            if (tid == kTpb - 32 && b + 2 < batches)
+                bulk_load(&S.rows[(b + 2) % 3][0][0], a.rt + (int64_t)(T.v0 + kBatchRows * (b + 2)) * kRowWords,
+                          kBatchBytes, &S.rows_bar[(b + 2) % 3]);
 
-            // ---- counter: batch b from ring[buf] ----------------------------------------------
-            const int hs = b % 5;
+            // ---- counter: the two strips of batch b from ring[buf] ---------------------------
 #pragma unroll
-            for (int k = 0; k < kSlots; ++k) {
-                const int combo = warp + kWarps * k;
-                if (combo >= ncombo) break;  // warp-uniform
-                const int m = combo >> 1;
-                uint32_t n[4];
-#pragma unroll
-                for (int q = 0; q < 4; ++q) {
-                    const uint32_t* rec = &S.ring[buf][q][lane][0];
-                    const uint32_t keep = ((S.rvalid[rb][q] >> m) & 1u) ? cm[k] : 0u;
-                    n[q] = nibble_counts(rec[m] & (rec[kSwPlane] ^ fx[k]) & keep);
-                }
-                const uint32_t n01 = n[0] + n[1], n23 = n[2] + n[3];
-                const uint32_t e = (n01 & 0x0F0F0F0Fu) + (n23 & 0x0F0F0F0Fu);
-                const uint32_t o = ((n01 >> 4) & 0x0F0F0F0Fu) + ((n23 >> 4) & 0x0F0F0F0Fu);
-                uint32_t en = __shfl_down_sync(kFull, e, 1), on = __shfl_down_sync(kFull, o, 1);
-                if (lane == kWords - 1) en = on = 0;
-                const uint32_t s = e + o, sn = en + on;
-                const uint32_t s1 = __funnelshift_r(s, sn, 8);
-                const uint32_t ge = s + s1 + __funnelshift_r(e, en, 16);
-                const uint32_t go = o + s1 + __funnelshift_r(s, sn, 16);
-                guard |= (ge + 0x4C4C4C4Cu) | (go + 0x4C4C4C4Cu);
-                re[k] += ge - S.hist_e[hs][combo][lane];
-                ro[k] += go - S.hist_o[hs][combo][lane];
-                S.hist_e[hs][combo][lane] = ge;
-                S.hist_o[hs][combo][lane] = go;
-                // hist_n[hs] held batch b-5; batch b-4 is in slot (b+1)%5.
-                const uint32_t top01 = S.hist_n[(b + 1) % 5][combo][lane];
-                S.hist_n[hs][combo][lane] = n01;
-                uint32_t flag = 0;
-                if (b >= 4) {
-                    const uint32_t te = bytes_at_least(re[k], thr4), to = bytes_at_least(ro[k], thr4);
-                    flag = te | (to >> 1);  // even groups at bits 8k+7, odd at 8k+6
-                    if (lane == kWords - 1) flag &= 0x0000C0C0u;  // groups 4..7: centres >= 1,008
-                }
-                // Second test of flagged groups: drop the 8 outer cells of rows 0, 1 (batch b-4)
-                // and rows 18, 19 (batch b), which no window of the group reaches.
-                const uint32_t top01n = __shfl_down_sync(kFull, top01, 1);
-                const uint32_t n23n = __shfl_down_sync(kFull, n23, 1);
-                if (flag) {
-                    const uint64_t t01 = ((uint64_t)(lane == kWords - 1 ? 0u : top01n) << 32) | top01;
-                    const uint64_t b23 = ((uint64_t)(lane == kWords - 1 ? 0u : n23n) << 32) | n23;
-                    uint32_t gm = 0;
-#pragma unroll
-                    for (int g = 0; g < 8; ++g) {
-                        const int bit = (g & 1) ? 8 * (g >> 1) + 6 : 8 * (g >> 1) + 7;
-                        if (!((flag >> bit) & 1u)) continue;
-                        const uint32_t box = (((g & 1) ? ro[k] : re[k]) >> (8 * (g >> 1))) & 0xFFu;
-                        const uint32_t outer = (uint32_t)((t01 >> (4 * g)) & 0xF) + (uint32_t)((t01 >> (4 * g + 16)) & 0xF) +
-                                               (uint32_t)((b23 >> (4 * g)) & 0xF) + (uint32_t)((b23 >> (4 * g + 16)) & 0xF);
-                        // A box byte of 128+ is a conservative report: keep the group.
-                        if (box >= 128u || box - outer >= (uint32_t)a.min_size) gm |= 1u << g;
-                    }
-                    pend[k] = push_groups(S, combo, lane, gm, b);
-                    pend_b[k] = b;
-                }
+            for (int t = 0; t < 2; ++t) {
+                if (interior)
+                    count_strip<false>(S, a, C, buf, rb, t, 2 * b + t, warp, lane, ncombo, thr4, guard);
+                else
+                    count_strip<true>(S, a, C, buf, rb, t, 2 * b + t, warp, lane, ncombo, thr4, guard);
             }
         }
         __syncthreads();
-        drain_queue(S, a, T, tid, warp, lane, pend, pend_b, true);
+        drain_queue(S, a, T, tid, warp, lane, C, true);
     }
     // A 4-row strip with 52+ hits among its 80 cells could carry a box past a byte lane.
     if (guard & 0x80808080u) atomicOr(a.overflow, 1u);
 }
 
-// rt[v * stride + 0] = low 17 bits of the row term of base row v; rt[v * stride + 1 + j] = its
-// high part (>> 17) in band j, for base rows v < vrows and bands j < nj (0 outside the area).
-__global__ void row_terms_kernel(uint32_t* rt, int32_t stride, int32_t vrows, int32_t nj,
+// Row-term table, one record of kRowWords words per (band group g, base row v), records of a
+// group contiguous: [m] = high part (>> 17) of the row term in band 32g + m (0 where the row lies
+// outside the area plus halo), [kRowLo] = its low 17 bits, [kRowValid] = number of bands of the
+// group that hold the row. Rows v >= vrows (padding) are all zero.
+__global__ void row_terms_kernel(uint32_t* rt, int32_t vrows_alloc, int32_t vrows, int32_t nj,
                                  int32_t first, int64_t limit, int64_t seed, int32_t use_x_term) {
+    const int32_t groups = (nj + kMaxBands - 1) / kMaxBands;
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= (int64_t)vrows * nj) return;
-    const int32_t v = (int32_t)(e / nj), j = (int32_t)(e % nj);
-    const int64_t off = (int64_t)v + (int64_t)j * kPeriod;
-    uint64_t t = 0;
-    if (off < limit) {
-        const int32_t c = (int32_t)((int64_t)first + off);
-        t = use_x_term ? x_term(c) + (uint64_t)seed : z_term(c) + (uint64_t)seed;
+    if (e >= (int64_t)groups * vrows_alloc * kRowWords) return;
+    const int32_t w = (int32_t)(e % kRowWords);
+    const int64_t rec = e / kRowWords;
+    const int32_t v = (int32_t)(rec % vrows_alloc), g = (int32_t)(rec / vrows_alloc);
+    uint32_t out = 0;
+    if (v < vrows) {
+        if (w < kMaxBands || w == kRowLo) {
+            const int32_t j = w == kRowLo ? 0 : g * kMaxBands + w;
+            const int64_t off = (int64_t)v + (int64_t)j * kPeriod;
+            if (j < nj && off < limit) {
+                const int32_t c = (int32_t)((int64_t)first + off);
+                const uint64_t t = (use_x_term ? x_term(c) : z_term(c)) + (uint64_t)seed;
+                out = w == kRowLo ? (uint32_t)t & 0x1FFFFu : (uint32_t)(t >> kPeriodBits);
+            }
+        } else if (w == kRowValid) {
+            // bands j = 32g + m with v + j * 2^17 < limit, capped at the group's size
+            const int64_t jmax = (limit - 1 - v) / kPeriod;  // last band holding the row
+            const int64_t n = min((int64_t)nj, jmax + 1) - (int64_t)g * kMaxBands;
+            out = (uint32_t)max((int64_t)0, min((int64_t)kMaxBands, n));
+        }
     }
-    if (j == 0) rt[(int64_t)v * stride] = (uint32_t)t & 0x1FFFFu;
-    rt[(int64_t)v * stride + 1 + j] = (uint32_t)(t >> kPeriodBits);
+    rt[e] = out;
 }
 
 __global__ void col_terms_kernel(uint64_t* ct, int32_t first, int32_t n, int32_t use_x_term) {
@@ -436,13 +526,16 @@ cudaError_t launch_band_scan(const BandArgs& a, int grid, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+int band_row_words() { return kRowWords; }
+
 cudaError_t launch_band_terms(uint64_t* ct, int32_t col_first, int32_t ncols, uint32_t* rt,
-                              int32_t rstride, int32_t vrows, int32_t nj, int32_t row_first,
+                              int32_t vrows_alloc, int32_t vrows, int32_t nj, int32_t row_first,
                               int64_t row_limit, int64_t seed, bool transposed, cudaStream_t s) {
     // Columns carry no seed; rows carry it. Transposed searches swap which axis is x.
     col_terms_kernel<<<(ncols + 255) / 256, 256, 0, s>>>(ct, col_first, ncols, transposed ? 0 : 1);
-    const int64_t n = (int64_t)vrows * nj;
-    row_terms_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(rt, rstride, vrows, nj, row_first,
+    const int64_t groups = (nj + kMaxBands - 1) / kMaxBands;
+    const int64_t n = groups * vrows_alloc * kRowWords;
+    row_terms_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(rt, vrows_alloc, vrows, nj, row_first,
                                                                 row_limit, seed, transposed ? 1 : 0);
     return cudaGetLastError();
 }
