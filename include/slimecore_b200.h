@@ -143,6 +143,23 @@ int32_t slime_b200_is_slime_batch(int64_t seed, const int64_t* x, const int64_t*
  * timed milliseconds. Returns 0, or -1 on a CUDA failure. */
 int32_t slime_b200_microbench(int32_t kind, int32_t iters, double* lane_ops_per_s, double* ms);
 
+/* Search without any allocation (no counterpart in the reference). For callers that cannot
+ * allocate GPU memory while they search -- an application whose own pool or caching allocator
+ * owns the device memory, a service that must not take cudaMalloc's implicit device
+ * synchronisation on its request path, or a program with a fixed memory budget. Same arguments,
+ * return value and ranked output as search_slime_clusters_gpu_v1_centered, without precise
+ * scoring. Its working memory is one fixed 4 MiB array inside the library, which every GPU that
+ * loads the library holds until the process exits; the call makes no cudaMalloc, cudaFree,
+ * cudaMallocHost or host heap allocation. Limits: rd_max <= 8191 and max_results <= 65536;
+ * larger requests return -1 with an error text (slime_b200_last_error). The first call on a
+ * device looks up the array's device address (set-up), so make that first call before any
+ * stream capture. All calls share the array: calls that overlap on the GPU (for example from
+ * several processes or contexts on one device at once) race; calls from one process are
+ * serialised. Runs on the legacy default stream. */
+int64_t slime_b200_search_noalloc(int64_t seed, int64_t rd_max, int32_t min_size, int32_t max_size,
+                                  int64_t rd_min, int32_t search_center_x, int32_t search_center_z,
+                                  ExtChunkResult* results_buffer, int32_t max_results);
+
 #ifdef __cplusplus
 }
 #endif
