@@ -99,7 +99,7 @@ __global__ void __launch_bounds__(256) fixup_kernel(const int2* rare, int32_t nr
         const int32_t cx = rc.x + dx, cz = rc.y + dz;
         bool owned = true;
         for (int k = 0; k < near_n; ++k) {
-            const int ox = cx - near[k].x, oz = cz - near[k].y;
+            const int64_t ox = (int64_t)cx - near[k].x, oz = (int64_t)cz - near[k].y;
             if (ox * ox + oz * oz <= 68) owned = false;
         }
         if (!owned) continue;
@@ -125,7 +125,8 @@ __global__ void filter_hits_kernel(Hit* hits, int64_t n, const int2* rs, int32_t
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const Hit h = hits[i];
         for (int k = 0; k < nrare; ++k) {
-            const int dx = h.cx - rs[k].x, dz = h.cz - rs[k].y;
+            // 64-bit: centres and rare chunks can lie millions of chunks apart.
+            const int64_t dx = (int64_t)h.cx - rs[k].x, dz = (int64_t)h.cz - rs[k].y;
             if (dx * dx + dz * dz <= 68) {
                 hits[i].count = -1;
                 break;

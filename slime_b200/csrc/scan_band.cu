@@ -59,8 +59,10 @@ struct __align__(16) BandSmem {
     unsigned long long rows_bar[3];           // mbarriers of the three row-term buffers
     uint32_t queue[kQueueCap];                // combo << 24 | word << 19 | group << 16 | strip
     uint32_t scratch[kWarps][20];             // re-evaluation rows, one block per warp
+    uint8_t pend[2][kMaxCombos][kWords];      // flagged groups of the last counted batch (per
+                                              // strip, combo and word) that did not fit in the queue
     int qcount;
-    int qover;
+    int qover;   // some flagged group is pending
     int failed;  // a bounded wait gave up: the CTA stops
 };
 
@@ -186,114 +188,117 @@ __device__ void flush_queue(BandSmem& S, const BandArgs& a, const Tile& T, int w
     }
 }
 
-// Per-thread counter state: one entry per combo slot of the warp (lane = word).
+// Per-thread counter state: one entry per combo slot of the warp (lane = word). The combo of
+// slot k is warp + 16 k, so all four slots of a warp share one phase and one swap sense.
 struct Counter {
-    uint32_t cm[kSlots];      // columns of the word that exist for the slot's phase
-    uint32_t fx[kSlots];      // ~0 where the swap ballot is inverted to select the combo's phase
+    uint32_t cm[kSlots];              // columns of the word that exist for the slot's phase
     uint32_t re[kSlots], ro[kSlots];  // rolling 20x20 boxes (even / odd groups, byte lanes)
-    uint32_t pend[kSlots][2]; // flagged groups that did not fit in the queue, per strip of the
-    int pend_s[kSlots][2];    // batch (all are re-pushed before the next batch is counted)
 };
 
-// Counts one 4-row strip (rows r0..r0+3 of ring[buf]) for every combo slot of this warp:
-// 4x4 block counts, 20-column strip sums, rolling 20x20 boxes, threshold test, the trimmed
-// second test of flagged groups, and queueing of the survivors.
-template <bool kMasked>
-__device__ __forceinline__ void count_strip(BandSmem& S, const BandArgs& a, Counter& C, int buf,
-                                            int rb, int t, int st, int warp, int lane, int ncombo,
-                                            uint32_t thr4, uint32_t& guard) {
-    const int r0 = 4 * t;  // t is a compile-time constant after unrolling: static register indexing
-    const int hs = st % 5;
-    uint32_t rvalid[4];
-    if (kMasked) {
-#pragma unroll
-        for (int q = 0; q < 4; ++q) {
-            const uint32_t nv = S.rows[rb][r0 + q][kRowValid];
-            rvalid[q] = nv >= 32 ? ~0u : (1u << nv) - 1u;
+// Second test of the flagged groups of one combo, all 8 groups at once in byte lanes: the 8
+// outer cells of rows 0, 1 (strip st - 4) and of rows 18, 19 (strip st), which no window of the
+// group reaches, are removed from the box (368 cells remain; the box bytes are exact, so no byte
+// borrows). Survivors go to the queue; those that do not fit are kept in S.pend.
+__device__ __forceinline__ void second_test(BandSmem& S, uint32_t flag, uint32_t re, uint32_t ro, uint32_t n23,
+                                            uint32_t thr4, int combo, int lane, int st, int t) {
+    const uint32_t top01 = S.hist_n[(st + 1) % 5][combo][lane];  // rows 0+1 of strip st - 4
+    // Outer cells of group g: 4-column blocks g and g + 4 of those four rows (byte lanes as in
+    // the boxes: even groups from even blocks, odd groups from odd blocks).
+    const uint32_t E = (top01 & 0x0F0F0F0Fu) + (n23 & 0x0F0F0F0Fu);
+    const uint32_t O = ((top01 >> 4) & 0x0F0F0F0Fu) + ((n23 >> 4) & 0x0F0F0F0Fu);
+    // Lane 31 reads its own words here; only its groups 0..3 (which use no neighbour) can flag.
+    const uint32_t En = __shfl_down_sync(kFull, E, 1), On = __shfl_down_sync(kFull, O, 1);
+    const uint32_t oe = E + __funnelshift_r(E, En, 16), oo = O + __funnelshift_r(O, On, 16);
+    const uint32_t f2 = (bytes_at_least(re - oe, thr4) | (bytes_at_least(ro - oo, thr4) >> 1)) & flag;
+    if (f2) {
+        uint32_t gm = 0;  // bit 8j+7 -> group 2j, bit 8j+6 -> group 2j+1
+        for (uint32_t f = f2; f; f &= f - 1) {
+            const int bit = __ffs(f) - 1;
+            gm |= 1u << (2 * (bit >> 3) + 7 - (bit & 7));
         }
-    }
-#pragma unroll
-    for (int k = 0; k < kSlots; ++k) {
-        const int combo = warp + kWarps * k;
-        if (combo < ncombo) {  // warp-uniform
-            const int m = combo >> 1;
-            uint32_t n[4];
-#pragma unroll
-            for (int q = 0; q < 4; ++q) {
-                uint32_t w = S.ring[buf][r0 + q][m][lane] & (S.ring[buf][r0 + q][kSwPlane][lane] ^ C.fx[k]);
-                if (kMasked) w &= ((rvalid[q] >> m) & 1u) ? C.cm[k] : 0u;
-                n[q] = nibble_counts(w);
-            }
-            const uint32_t n01 = n[0] + n[1], n23 = n[2] + n[3];
-            const uint32_t e = (n01 & 0x0F0F0F0Fu) + (n23 & 0x0F0F0F0Fu);
-            const uint32_t o = ((n01 >> 4) & 0x0F0F0F0Fu) + ((n23 >> 4) & 0x0F0F0F0Fu);
-            uint32_t en = __shfl_down_sync(kFull, e, 1), on = __shfl_down_sync(kFull, o, 1);
-            if (lane == kWords - 1) en = on = 0;
-            const uint32_t s = e + o, sn = en + on;
-            const uint32_t s1 = __funnelshift_r(s, sn, 8);
-            const uint32_t ge = s + s1 + __funnelshift_r(e, en, 16);
-            const uint32_t go = o + s1 + __funnelshift_r(s, sn, 16);
-            guard |= (ge + 0x4C4C4C4Cu) | (go + 0x4C4C4C4Cu);
-            uint32_t* he = &S.hist_e[hs][combo][lane];
-            uint32_t* ho = &S.hist_o[hs][combo][lane];
-            C.re[k] += ge - *he;
-            C.ro[k] += go - *ho;
-            *he = ge;
-            *ho = go;
-            S.hist_n[hs][combo][lane] = n01;
-            uint32_t flag = 0;
-            if (st >= 4) {
-                const uint32_t te = bytes_at_least(C.re[k], thr4), to = bytes_at_least(C.ro[k], thr4);
-                flag = te | (to >> 1);  // even groups at bits 8k+7, odd at 8k+6
-                if (lane == kWords - 1) flag &= 0x0000C0C0u;  // groups 4..7: centres >= 1,008
-            }
-            // Second test of flagged groups: drop the 8 outer cells of rows 0, 1 (strip st-4) and
-            // rows 18, 19 (strip st), which no window of the group reaches.
-            if (__any_sync(kFull, flag != 0)) {
-                const uint32_t top01 = S.hist_n[(st + 1) % 5][combo][lane];  // strip st - 4
-                const uint32_t top01n = __shfl_down_sync(kFull, top01, 1);
-                const uint32_t n23n = __shfl_down_sync(kFull, n23, 1);
-                if (flag) {
-                    const uint64_t t01 = ((uint64_t)(lane == kWords - 1 ? 0u : top01n) << 32) | top01;
-                    const uint64_t b23 = ((uint64_t)(lane == kWords - 1 ? 0u : n23n) << 32) | n23;
-                    uint32_t gm = 0;
-#pragma unroll
-                    for (int g = 0; g < 8; ++g) {
-                        const int bit = (g & 1) ? 8 * (g >> 1) + 6 : 8 * (g >> 1) + 7;
-                        if (!((flag >> bit) & 1u)) continue;
-                        const uint32_t box = (((g & 1) ? C.ro[k] : C.re[k]) >> (8 * (g >> 1))) & 0xFFu;
-                        const uint32_t outer = (uint32_t)((t01 >> (4 * g)) & 0xF) + (uint32_t)((t01 >> (4 * g + 16)) & 0xF) +
-                                               (uint32_t)((b23 >> (4 * g)) & 0xF) + (uint32_t)((b23 >> (4 * g + 16)) & 0xF);
-                        // A box byte of 128+ is a conservative report: keep the group.
-                        if (box >= 128u || box - outer >= (uint32_t)a.min_size) gm |= 1u << g;
-                    }
-                    if (gm) {
-                        C.pend[k][t] = push_groups(S, combo, lane, gm, st);
-                        C.pend_s[k][t] = st;
-                    }
-                }
-            }
-        }
+        const uint32_t left = push_groups(S, combo, lane, gm, st);
+        if (left) S.pend[t][combo][lane] = (uint8_t)left;
     }
 }
 
-// Processes the queue (all threads; block-uniform entry) and re-pushes pending groups. With
-// `final` it repeats until queue and pending groups are empty; otherwise it may return with a
-// partial queue (fewer than kQueueFlush groups) and no pending groups.
+// Counts one 4-row strip (rows 4t..4t+3 of ring[buf]) for the warp's four combo slots as one
+// straight-line block: 4x4 block counts, 20-column strip sums, rolling 20x20 boxes and the
+// threshold test. Only when a lane flags a group does the warp take the second test. Slots of
+// combos beyond the launch's band count read zero planes and never flag.
+template <bool kMasked>
+__device__ __forceinline__ void count_strip(BandSmem& S, const BandArgs& a, Counter& C, int buf, int t,
+                                            int st, int warp, int lane, uint32_t fx, uint32_t lastmask,
+                                            uint32_t thr4, uint32_t& guard) {
+    const int r0 = 4 * t;  // t is a compile-time constant after unrolling
+    const int hs = st % 5;
+    const uint32_t live = st >= 4 ? lastmask : 0u;  // boxes are complete from the fifth strip on
+    uint32_t sel[4];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) sel[q] = S.ring[buf][r0 + q][kSwPlane][lane] ^ fx;
+    uint32_t fl[kSlots], n23s[kSlots];
+    uint32_t any = 0;
+#pragma unroll
+    for (int k = 0; k < kSlots; ++k) {
+        const int combo = warp + kWarps * k;
+        const int m = combo >> 1;
+        uint32_t n[4];
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            uint32_t w = S.ring[buf][r0 + q][m][lane] & sel[q];
+            if (kMasked) w &= C.cm[k];
+            n[q] = nibble_counts(w);
+        }
+        const uint32_t n01 = n[0] + n[1], n23 = n[2] + n[3];
+        const uint32_t e = (n01 & 0x0F0F0F0Fu) + (n23 & 0x0F0F0F0Fu);
+        const uint32_t o = ((n01 >> 4) & 0x0F0F0F0Fu) + ((n23 >> 4) & 0x0F0F0F0Fu);
+        // Lane 31 gets its own words back: they feed only groups 4..7, which it never flags.
+        const uint32_t en = __shfl_down_sync(kFull, e, 1), on = __shfl_down_sync(kFull, o, 1);
+        const uint32_t s = e + o, sn = en + on;
+        const uint32_t s1 = __funnelshift_r(s, sn, 8);
+        const uint32_t ge = s + s1 + __funnelshift_r(e, en, 16);
+        const uint32_t go = o + s1 + __funnelshift_r(s, sn, 16);
+        guard |= (ge + 0x4C4C4C4Cu) | (go + 0x4C4C4C4Cu);
+        uint32_t* he = &S.hist_e[hs][combo][lane];
+        uint32_t* ho = &S.hist_o[hs][combo][lane];
+        C.re[k] += ge - *he;
+        C.ro[k] += go - *ho;
+        *he = ge;
+        *ho = go;
+        S.hist_n[hs][combo][lane] = n01;
+        const uint32_t te = bytes_at_least(C.re[k], thr4), to = bytes_at_least(C.ro[k], thr4);
+        fl[k] = (te | (to >> 1)) & live;  // even groups at bits 8j+7, odd groups at 8j+6
+        n23s[k] = n23;
+        any |= fl[k];
+    }
+    if (__any_sync(kFull, any != 0)) {
+#pragma unroll
+        for (int k = 0; k < kSlots; ++k)
+            if (__any_sync(kFull, fl[k] != 0))
+                second_test(S, fl[k], C.re[k], C.ro[k], n23s[k], thr4, warp + kWarps * k, lane, st, t);
+    }
+}
+
+// Processes the queue (all threads; block-uniform entry) and re-pushes pending groups of batch
+// `bprev`. With `final` it repeats until queue and pending groups are empty; otherwise it may
+// return with a partial queue (fewer than kQueueFlush groups) and no pending groups.
 __device__ __forceinline__ void drain_queue(BandSmem& S, const BandArgs& a, const Tile& T, int tid, int warp,
-                            int lane, Counter& C, bool final) {
+                                            int lane, int bprev, bool final) {
     for (;;) {
         flush_queue(S, a, T, warp, lane);
-        __syncthreads();
+        const bool over = __syncthreads_or(S.qover != 0);
         if (tid == 0) { S.qcount = 0; S.qover = 0; }
         __syncthreads();
         bool left = false;
-#pragma unroll
-        for (int k = 0; k < kSlots; ++k) {
-#pragma unroll
-            for (int t = 0; t < 2; ++t) {
-                if (C.pend[k][t]) C.pend[k][t] = push_groups(S, warp + kWarps * k, lane, C.pend[k][t], C.pend_s[k][t]);
-                left |= C.pend[k][t] != 0;
+        if (over) {
+            for (int i = tid; i < 2 * kMaxCombos * kWords; i += kTpb) {
+                uint8_t* p = &S.pend[0][0][0] + i;
+                const uint32_t gm = *p;
+                if (gm) {
+                    const int t = i / (kMaxCombos * kWords), combo = (i / kWords) % kMaxCombos;
+                    const uint32_t rest = push_groups(S, combo, i % kWords, gm, 2 * bprev + t);
+                    *p = (uint8_t)rest;
+                    left |= rest != 0;
+                }
             }
         }
         const bool more = __syncthreads_or(left);
@@ -307,8 +312,9 @@ template <bool kMadAdd>
 __global__ void __launch_bounds__(kTpb, 1) band_scan_kernel(const BandArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     BandSmem& S = *reinterpret_cast<BandSmem*>(smem_raw);
-    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int nb = a.nb, ncombo = 2 * nb;
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int warp = __shfl_sync(kFull, tid >> 5, 0);  // warp-uniform for the compiler
+    const int nb = a.nb;
     const uint32_t thr4 = (uint32_t)min(a.min_size, 128) * 0x01010101u;
     const uint32_t one = a.one;  // 1 at run time: keeps the band add on the multiply pipe
     uint32_t guard = 0;
@@ -321,6 +327,13 @@ __global__ void __launch_bounds__(kTpb, 1) band_scan_kernel(const BandArgs a) {
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&S.rows_bar[r])) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
+    // Planes of bands beyond nb are never generated: they stay zero and count nothing.
+    for (int i = tid; i < 2 * kBatchRows * kPlanes * kWords; i += kTpb) (&S.ring[0][0][0][0])[i] = 0;
+    for (int i = tid; i < 2 * kMaxCombos * kWords; i += kTpb) (&S.pend[0][0][0])[i] = 0;
+    // Counter constants: the swap sense of the warp's phase and the groups lane 31 may flag
+    // (groups 4..7 of word 31 hold centres 1,008+ of the tile, which belong to the next tile).
+    const uint32_t fx = ((warp ^ (warp >> 1)) & 1) ? 0u : ~0u;
+    const uint32_t lastmask = lane == kWords - 1 ? 0x0000C0C0u : ~0u;
     __syncthreads();
 
     for (int64_t tile = a.tile_begin + blockIdx.x; tile < a.tile_end; tile += gridDim.x) {
@@ -362,17 +375,11 @@ __global__ void __launch_bounds__(kTpb, 1) band_scan_kernel(const BandArgs a) {
             const int64_t first = (int64_t)T.u0 + lane * 32 + (int64_t)(T.i0 + (combo & 1)) * kPeriod;
             const int64_t nvalid = a.ncols - first;
             C.cm[k] = nvalid >= 32 ? ~0u : nvalid <= 0 ? 0u : (1u << nvalid) - 1u;
-            C.fx[k] = ((combo ^ (combo >> 1)) & 1) ? 0u : ~0u;
             C.re[k] = C.ro[k] = 0;
-            C.pend[k][0] = C.pend[k][1] = 0;
-            C.pend_s[k][0] = C.pend_s[k][1] = 0;
         }
-        // Interior tiles (every column of both phases and every row of every band exists) skip
-        // the validity masks (block-uniform).
-        const bool interior =
-            (int64_t)T.u0 + kWords * 32 + (int64_t)(T.i0 + 1) * kPeriod <= a.ncols &&
-            (int64_t)T.v0 + (int64_t)batches * kBatchRows + (int64_t)(a.j0 + nb - 1) * kPeriod <= a.height_v + 16 &&
-            T.v0 + batches * kBatchRows <= a.vrows;
+        // Tiles whose columns all exist in both phases skip the column masks (block-uniform).
+        // Rows need no mask: the generator writes zero words for bands that do not hold a row.
+        const bool interior = (int64_t)T.u0 + kWords * 32 + (int64_t)(T.i0 + 1) * kPeriod <= a.ncols;
         for (int i = tid; i < 5 * kMaxCombos * kWords; i += kTpb) {
             (&S.hist_e[0][0][0])[i] = 0;
             (&S.hist_o[0][0][0])[i] = 0;
@@ -399,6 +406,9 @@ __global__ void __launch_bounds__(kTpb, 1) band_scan_kernel(const BandArgs a) {
                 const int q = gq + qq;
                 const uint32_t* zr = &S.rows[rb][q][0];
                 const uint32_t zlo = zr[kRowLo];
+                // Bands 0..nv-1 hold this row. The broadcast tells the compiler that the value
+                // (and the loops it bounds) is warp-uniform.
+                const int nv = __shfl_sync(kFull, min((int)zr[kRowValid], nb), 0);
                 const uint32_t zpar = (zr[0] ^ kXorHi) & 1u;
                 uint32_t xa[4], xb[4], dd[4], sw[4];
 #pragma unroll
@@ -410,32 +420,42 @@ __global__ void __launch_bounds__(kTpb, 1) band_scan_kernel(const BandArgs a) {
                     dd[k] = sh.d;
                     sw[k] = __ballot_sync(kFull, pi != 0);
                 }
-                uint32_t* dst = &S.ring[buf][q][0][gw];  // plane m at dst + m * kWords, 16-byte aligned
-                if (lane == 0) *reinterpret_cast<uint4*>(dst + kSwPlane * kWords) = make_uint4(sw[0], sw[1], sw[2], sw[3]);
+                // Plane m of the warp's 4 words at dst + m * kWords (16-byte aligned). Every lane
+                // stores the same ballot words to the same address: no predicate, no branch.
+                uint4* dst = reinterpret_cast<uint4*>(&S.ring[buf][q][0][gw]);
+                constexpr int kPlaneStep = kWords / 4;  // uint4 per plane
+                dst[kSwPlane * kPlaneStep] = make_uint4(sw[0], sw[1], sw[2], sw[3]);
                 auto hit = [&](uint32_t x, uint32_t z, uint32_t d) {
                     const uint32_t t = kMadAdd ? z * one + x : z + x;
                     return ((t ^ kXorHi) * kMulH + d) < kHitBelow;
                 };
-                int m = 0;
-                for (; m + 1 < nb; m += 2) {
-                    const uint2 z2 = *reinterpret_cast<const uint2*>(zr + m);  // m even: aligned
-                    uint32_t wa[4], wb[4];
+                // Bands 0..count-1 of the row; returns count.
+                auto bands = [&](const int count) {
+                    int m = 0;
+                    for (; m + 1 < count; m += 2) {
+                        const uint2 z2 = *reinterpret_cast<const uint2*>(zr + m);  // m even: aligned
+                        uint32_t wa[4], wb[4];
 #pragma unroll
-                    for (int k = 0; k < 4; ++k) {
-                        wa[k] = __ballot_sync(kFull, hit(xa[k], z2.x, dd[k]));
-                        wb[k] = __ballot_sync(kFull, hit(xb[k], z2.y, dd[k]));
+                        for (int k = 0; k < 4; ++k) {
+                            wa[k] = __ballot_sync(kFull, hit(xa[k], z2.x, dd[k]));
+                            wb[k] = __ballot_sync(kFull, hit(xb[k], z2.y, dd[k]));
+                        }
+                        dst[m * kPlaneStep] = make_uint4(wa[0], wa[1], wa[2], wa[3]);
+                        dst[(m + 1) * kPlaneStep] = make_uint4(wb[0], wb[1], wb[2], wb[3]);
                     }
-                    if (lane == 0) {
-                        *reinterpret_cast<uint4*>(dst + m * kWords) = make_uint4(wa[0], wa[1], wa[2], wa[3]);
-                        *reinterpret_cast<uint4*>(dst + (m + 1) * kWords) = make_uint4(wb[0], wb[1], wb[2], wb[3]);
-                    }
-                }
-                if (m < nb) {  // odd band count: the last band uses the even-band phase choice
-                    const uint32_t z0 = zr[m];
-                    uint32_t wa[4];
+                    if (m < count) {  // odd count: the last band (m even) uses the even-band phase choice
+                        const uint32_t z0 = zr[m];
+                        uint32_t wa[4];
 #pragma unroll
-                    for (int k = 0; k < 4; ++k) wa[k] = __ballot_sync(kFull, hit(xa[k], z0, dd[k]));
-                    if (lane == 0) *reinterpret_cast<uint4*>(dst + m * kWords) = make_uint4(wa[0], wa[1], wa[2], wa[3]);
+                        for (int k = 0; k < 4; ++k) wa[k] = __ballot_sync(kFull, hit(xa[k], z0, dd[k]));
+                        dst[m * kPlaneStep] = make_uint4(wa[0], wa[1], wa[2], wa[3]);
+                    }
+                };
+                if (nv == nb) {
+                    bands(nb);  // the common case: the kernel-uniform band count bounds the loop
+                } else {
+                    bands(nv);
+                    for (int m = nv; m < nb; ++m) dst[m * kPlaneStep] = make_uint4(0u, 0u, 0u, 0u);  // rows outside band m
                 }
             }
             __syncthreads();
@@ -443,7 +463,7 @@ __global__ void __launch_bounds__(kTpb, 1) band_scan_kernel(const BandArgs a) {
 
             // ---- survivor queue: flush when half full; groups that did not fit are re-pushed ---
             if (S.qcount >= kQueueFlush || S.qover)
-                drain_queue(S, a, T, tid, warp, lane, C, false);
+                drain_queue(S, a, T, tid, warp, lane, b - 1, false);
             // Row terms of batch b + 2 (its buffer was last read before this batch's barrier).
             if (tid == kTpb - 32 && b + 2 < batches)
                 bulk_load(&S.rows[(b + 2) % 3][0][0], a.rt + (int64_t)(T.v0 + kBatchRows * (b + 2)) * kRowWords,
@@ -453,13 +473,13 @@ __global__ void __launch_bounds__(kTpb, 1) band_scan_kernel(const BandArgs a) {
 #pragma unroll
             for (int t = 0; t < 2; ++t) {
                 if (interior)
-                    count_strip<false>(S, a, C, buf, rb, t, 2 * b + t, warp, lane, ncombo, thr4, guard);
+                    count_strip<false>(S, a, C, buf, t, 2 * b + t, warp, lane, fx, lastmask, thr4, guard);
                 else
-                    count_strip<true>(S, a, C, buf, rb, t, 2 * b + t, warp, lane, ncombo, thr4, guard);
+                    count_strip<true>(S, a, C, buf, t, 2 * b + t, warp, lane, fx, lastmask, thr4, guard);
             }
         }
         __syncthreads();
-        drain_queue(S, a, T, tid, warp, lane, C, true);
+        drain_queue(S, a, T, tid, warp, lane, batches - 1, true);
     }
     // A 4-row strip with 52+ hits among its 80 cells could carry a box past a byte lane.
     if (guard & 0x80808080u) atomicOr(a.overflow, 1u);

@@ -115,6 +115,20 @@ def test_band_vs_general_medium(core, case):
     assert np.array_equal(r_b, r_g)
 
 
+def test_band_vs_general_low_threshold_millions_of_sites(core):
+    """Threshold 42 on a 280,001^2 area: 3.1 million sites, a survivor queue that overflows in
+    every tile, and ~30 rare chunks whose distance test to far-away sites must not wrap."""
+    from slime_b200 import workloads
+    seed = workloads.full_world_scan().seed
+    case = (seed, 140_000, 42, 221, 0, 0, 0, 4_000_000)
+    t_g, r_g = run(core, 1, *case)
+    t_b, r_b = run(core, 2, *case)
+    assert t_g > 3_000_000
+    assert core.lib.slime_b200_last_rare_chunks() > 0
+    assert t_b == t_g
+    assert np.array_equal(r_b, r_g)
+
+
 @pytest.mark.skipif(not REF_GPU_SO.exists(), reason="reference GPU library not built")
 def test_band_full_world_vs_reference_gpu(core):
     from oracle.oracle import RefGpu
