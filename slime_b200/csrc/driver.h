@@ -97,9 +97,10 @@ struct Context {
     DeviceBuffer<unsigned int> flags;  // [0] overflow, [1] fix-up error, [2] rare count
     bool band_ready = false;
     int32_t engine_override = 0;       // 0 auto, 1 general scan, 2 band engine
-    // Auto mode uses the band engine from this threshold: below it the survivor queue dominates
-    // and the general scan is faster (B200 crossover measured between 48 and 49).
-    int32_t band_min_threshold = 49;
+    // Auto mode uses the band engine from this threshold: below it the exact counts of the many
+    // surviving 4x4 groups dominate and the general scan is faster (B200 crossover measured
+    // between 45 and 48 on a 1,200,001^2 area).
+    int32_t band_min_threshold = 47;
     int64_t last_rare = 0;             // rare redraw chunks found by the last band search
     int64_t band_fallbacks = 0;        // band searches redone by the general scan
     int32_t band_mad_add = 1;          // generator variant: band adds on the multiply pipe

@@ -9,18 +9,17 @@
 //    position the low-17-bit work (carry, Q, D, parity) is done once; per band it costs one add,
 //    one xor, one multiply-add, one compare and one ballot for the two phases together, because
 //    the parity tells which of the two phases can be a first-draw slime chunk.
-//  * Rows advance in batches of 8 (two 4-row strips). Ballots of a batch go to one of two
-//    buffers, so one barrier per batch separates the generator (batch b+1) from the counter
-//    (batch b). Row terms arrive by TMA bulk copies two batches ahead.
+//  * Rows advance in batches of 8 (two 4-row strips). Ballots of batch b go to ring slot b % 4,
+//    so one barrier per batch separates the generator (batch b+1) from the counter (batch b),
+//    which reads batches b-2..b. Row terms arrive by TMA bulk copies two batches ahead.
 //  * Counting is SWAR in byte lanes on 4x4 centre groups. A warp owns a combo (phase, band) row
 //    with one lane per 32-column word: nibble popcounts of the 4 rows give 4x4 block counts,
 //    the neighbour word comes by shuffle, three funnel shifts and two adds give the 20-column
-//    strip sums of the word's 8 groups, and a rolling sum over 5 batches gives the 20x20 box of
-//    each group, which bounds its 16 windows. A flagged group is re-tested in registers with
+//    strip sums of the word's 8 groups, and a rolling sum over 5 strips gives the 20x20 box of
+//    each group, which bounds its 16 windows. A flagged group is re-tested in byte lanes with
 //    the 32 cells of rows 0, 1, 18 and 19 that lie outside every window removed (368 cells).
-//  * Groups that pass both go to a queue; the CTA re-evaluates queued groups from the term
-//    tables (one warp per group: 20 x 20 first-draw bits, 16 exact window counts) and appends
-//    the centres in range to the hit list.
+//  * The warp then counts the 16 windows of each surviving group exactly from the ring (the
+//    group's 20 rows are still there) and appends the centres in range to the hit list.
 #include "band_math.cuh"
 #include "engine.h"
 
@@ -38,31 +37,23 @@ constexpr int kSwPlane = kMaxBands;         // plane of the phase-swap ballot
 constexpr int kPlanes = kMaxBands + 1;      // band planes and the swap plane
 constexpr int kMaxCombos = 2 * kMaxBands;
 constexpr int kSlots = kMaxCombos / kWarps; // combo rows counted per warp
-constexpr int kQueueCap = 1024;
-constexpr int kQueueFlush = 512;
 constexpr unsigned kFull = 0xFFFFFFFFu;
 
 // Row-term record of one base row for one group of up to 32 bands (matches the global table
-// written by row_terms_kernel, so a batch of 4 rows is one contiguous 576-byte bulk copy).
+// written by row_terms_kernel, so a batch of 8 rows is one contiguous 1,152-byte bulk copy).
 constexpr int kRowWords = 36;
 constexpr int kRowLo = 32;      // low 17 bits of the row term (shared by all bands)
 constexpr int kRowValid = 33;   // bands of the group that hold this row (prefix count)
 
 constexpr int kBatchRows = 8;               // rows per barrier: two 4-row strips
+constexpr int kRingSlots = 4;               // batches b-2..b are read while b+1 is generated
 
 struct __align__(16) BandSmem {
-    uint32_t ring[2][kBatchRows][kPlanes][kWords];  // [buffer][row][band planes | swap][word]
+    uint32_t ring[kRingSlots][kBatchRows][kPlanes][kWords];  // [batch % 4][row][band planes | swap][word]
     uint32_t hist_e[5][kMaxCombos][kWords];   // strip sums of the last 5 strips (even groups)
     uint32_t hist_o[5][kMaxCombos][kWords];   // (odd groups)
-    uint32_t hist_n[5][kMaxCombos][kWords];   // nibble counts of rows 0+1 of the last 5 strips
     uint32_t rows[3][kBatchRows][kRowWords];  // row terms of 3 batches, filled by bulk copies
     unsigned long long rows_bar[3];           // mbarriers of the three row-term buffers
-    uint32_t queue[kQueueCap];                // combo << 24 | word << 19 | group << 16 | strip
-    uint32_t scratch[kWarps][20];             // re-evaluation rows, one block per warp
-    uint8_t pend[2][kMaxCombos][kWords];      // flagged groups of the last counted batch (per
-                                              // strip, combo and word) that did not fit in the queue
-    int qcount;
-    int qover;   // some flagged group is pending
     int failed;  // a bounded wait gave up: the CTA stops
 };
 
@@ -106,85 +97,77 @@ __device__ __forceinline__ uint32_t bytes_at_least(uint32_t v, uint32_t t4) {
     return (((v | 0x80808080u) - t4) | v) & 0x80808080u;
 }
 
-// Appends the groups of `gm` to the queue; returns those that did not fit (kept pending).
-__device__ __forceinline__ uint32_t push_groups(BandSmem& S, int combo, int word, uint32_t gm, int b) {
-    while (gm) {
-        const int g = __ffs(gm) - 1;
-        const int idx = atomicAdd(&S.qcount, 1);
-        if (idx >= kQueueCap) {
-            S.qover = 1;
-            return gm;
-        }
-        S.queue[idx] = ((uint32_t)combo << 24) | ((uint32_t)word << 19) | ((uint32_t)g << 16) | (uint32_t)b;
-        gm &= gm - 1;
-    }
-    return 0;
-}
-
 struct Tile {
     int u0, v0, i0, out_h;
 };
 
-// Re-evaluates the queued groups from the term tables and appends the centres in range.
-__device__ void flush_queue(BandSmem& S, const BandArgs& a, const Tile& T, int warp, int lane) {
-    const int n = min(S.qcount, kQueueCap);
-    const bool no_upper = a.max_size >= 221;
-    for (int s = warp; s < n; s += kWarps) {
-        const uint32_t rec = S.queue[s];
-        const int combo = (int)(rec >> 24), word = (int)((rec >> 19) & 31);
-        const int g = (int)((rec >> 16) & 7), st = (int)(rec & 0xFFFF);
-        const int ph = combo & 1, m = combo >> 1;
-        const int c0 = word * 32 + 4 * g;       // first window column (tile-relative input col)
-        const int r0 = 4 * (st - 4);            // first window row (tile-relative input row)
-        uint64_t xt = 0;
-        if (lane < 20) {
-            const int64_t idx = (int64_t)T.u0 + c0 + lane + (int64_t)(T.i0 + ph) * kPeriod;
-            xt = idx < a.ncols ? a.ct[idx] : 0;
+// Columns of word `word` that exist for phase `ph` of the tile (all ones inside the area).
+__device__ __forceinline__ uint32_t column_mask(const BandArgs& a, const Tile& T, int word, int ph) {
+    const int64_t first = (int64_t)T.u0 + word * 32 + (int64_t)(T.i0 + ph) * kPeriod;
+    const int64_t nvalid = a.ncols - first;
+    return nvalid >= 32 ? ~0u : nvalid <= 0 ? 0u : (1u << nvalid) - 1u;
+}
+
+// Bits of combo (ph, m) in ring row `r` (tile-relative input row), word `word`.
+__device__ __forceinline__ uint32_t combo_word(const BandSmem& S, int r, int m, uint32_t fx, int word) {
+    const int slot = (r >> 3) & (kRingSlots - 1), q = r & 7;
+    return S.ring[slot][q][m][word] & (S.ring[slot][q][kSwPlane][word] ^ fx);
+}
+
+// Exact window counts of the 16 centres of group g of word `word` for one combo, from the 20
+// ring rows of strips st-4..st. Lanes 0..19 fetch one 20-column row slice each; lanes 0..15 then
+// count one centre (dx = lane & 3, dz = lane >> 2) over 17 shuffled slices. Centres in range are
+// appended to the hit list. Warp-uniform arguments; called by the whole warp.
+template <bool kMasked>
+__device__ __forceinline__ void exact_group(const BandSmem& S, const BandArgs& a, const Tile& T, int combo,
+                                         uint32_t fx, int word, int g, int st, int lane) {
+    const int ph = combo & 1, m = combo >> 1;
+    const int c0 = word * 32 + 4 * g;       // first window column (tile-relative input col)
+    const int r0 = 4 * (st - 4);            // first window row (tile-relative input row)
+    uint32_t slice = 0;
+    if (lane < 20) {
+        uint32_t lo = combo_word(S, r0 + lane, m, fx, word);
+        uint32_t hi = word + 1 < kWords ? combo_word(S, r0 + lane, m, fx, word + 1) : 0u;
+        if (kMasked) {
+            lo &= column_mask(a, T, word, ph);
+            hi &= word + 1 < kWords ? column_mask(a, T, word + 1, ph) : 0u;
         }
-        for (int t = 0; t < 20; ++t) {
-            const int vi = T.v0 + r0 + t;
-            uint64_t zt = 0;
-            if (vi < a.vrows) {
-                const uint32_t* row = a.rt + (int64_t)vi * kRowWords;
-                zt = (uint64_t)row[kRowLo] | ((uint64_t)row[m] << kPeriodBits);
-            }
-            const uint32_t bits = __ballot_sync(kFull, lane < 20 && first_draw_slime(xt, zt));
-            if (lane == 0) S.scratch[warp][t] = bits;
-        }
-        __syncwarp();
-        bool keep = false;
-        int count = 0, cx = 0, cz = 0;
-        if (lane < 16) {
-            const int dx = lane & 3, dz = lane >> 2;
+        slice = __funnelshift_r(lo, hi, 4 * g) & 0xFFFFFu;
+    }
+    const int dx = lane & 3, dz = (lane >> 2) & 3;
+    int count = 0;
 #pragma unroll
-            for (int i = 0; i < 17; ++i)
-                count += __popc((S.scratch[warp][dz + i] >> dx) & window_row_mask(i));
-            const int c = c0 + dx, rr = r0 + dz;
-            const int64_t u = (int64_t)T.u0 + c, v = (int64_t)T.v0 + rr;
-            const int64_t cu = u + (int64_t)(T.i0 + ph) * kPeriod;
-            const int64_t cv = v + (int64_t)(a.j0 + m) * kPeriod;
-            keep = count >= a.min_size && (no_upper || count <= a.max_size) && c < kOutW &&
-                   u < a.ubase && rr < T.out_h && cu < a.width_u && cv < a.height_v;
-            if (keep) {
-                cx = (int32_t)(a.transposed ? a.area_x0 + cv : a.area_x0 + cu);
-                cz = (int32_t)(a.transposed ? a.area_z0 + cu : a.area_z0 + cv);
-                if (a.rd_min_sq) {
-                    const int64_t ddx = (int64_t)cx - a.center_x, ddz = (int64_t)cz - a.center_z;
-                    keep = ddx * ddx + ddz * ddz >= a.rd_min_sq;
-                }
+    for (int i = 0; i < 17; ++i) {
+        const uint32_t row = __shfl_sync(kFull, slice, dz + i);
+        count += __popc((row >> dx) & window_row_mask(i));
+    }
+    bool keep = false;
+    int cx = 0, cz = 0;
+    if (lane < 16) {
+        const int c = c0 + dx, rr = r0 + dz;
+        const int64_t u = (int64_t)T.u0 + c, v = (int64_t)T.v0 + rr;
+        const int64_t cu = u + (int64_t)(T.i0 + ph) * kPeriod;
+        const int64_t cv = v + (int64_t)(a.j0 + m) * kPeriod;
+        keep = count >= a.min_size && count <= a.max_size && c < kOutW && u < a.ubase &&
+               rr < T.out_h && cu < a.width_u && cv < a.height_v;
+        if (keep) {
+            cx = (int32_t)(a.transposed ? a.area_x0 + cv : a.area_x0 + cu);
+            cz = (int32_t)(a.transposed ? a.area_z0 + cu : a.area_z0 + cv);
+            if (a.rd_min_sq) {
+                const int64_t ddx = (int64_t)cx - a.center_x, ddz = (int64_t)cz - a.center_z;
+                keep = ddx * ddx + ddz * ddz >= a.rd_min_sq;
             }
         }
-        const unsigned mk = __ballot_sync(kFull, keep);
-        if (mk) {
-            unsigned long long base = 0;
-            if (lane == 0) base = atomicAdd(a.emitted, (unsigned long long)__popc(mk));
-            base = __shfl_sync(kFull, base, 0);
-            if (keep) {
-                const unsigned long long idx = base + __popc(mk & ((1u << lane) - 1u));
-                if (idx < a.cap) a.out[idx] = Hit{count, cx, cz};
-            }
+    }
+    const unsigned mk = __ballot_sync(kFull, keep);
+    if (mk) {
+        unsigned long long base = 0;
+        if (lane == 0) base = atomicAdd(a.emitted, (unsigned long long)__popc(mk));
+        base = __shfl_sync(kFull, base, 0);
+        if (keep) {
+            const unsigned long long idx = base + __popc(mk & ((1u << lane) - 1u));
+            if (idx < a.cap) a.out[idx] = Hit{count, cx, cz};
         }
-        __syncwarp();
     }
 }
 
@@ -198,10 +181,16 @@ struct Counter {
 // Second test of the flagged groups of one combo, all 8 groups at once in byte lanes: the 8
 // outer cells of rows 0, 1 (strip st - 4) and of rows 18, 19 (strip st), which no window of the
 // group reaches, are removed from the box (368 cells remain; the box bytes are exact, so no byte
-// borrows). Survivors go to the queue; those that do not fit are kept in S.pend.
-__device__ __forceinline__ void second_test(BandSmem& S, uint32_t flag, uint32_t re, uint32_t ro, uint32_t n23,
-                                            uint32_t thr4, int combo, int lane, int st, int t) {
-    const uint32_t top01 = S.hist_n[(st + 1) % 5][combo][lane];  // rows 0+1 of strip st - 4
+// borrows). Survivors are counted exactly. Called by the whole warp.
+template <bool kMasked>
+__device__ __forceinline__ void second_test(const BandSmem& S, const BandArgs& a, const Tile& T, uint32_t flag,
+                                            uint32_t re, uint32_t ro, uint32_t n23, uint32_t cm, uint32_t fx,
+                                            uint32_t thr4, int combo, int lane, int st) {
+    const int m = combo >> 1;
+    const int r0 = 4 * (st - 4);  // rows 0 and 1 of strip st - 4
+    uint32_t w0 = combo_word(S, r0, m, fx, lane), w1 = combo_word(S, r0 + 1, m, fx, lane);
+    if (kMasked) { w0 &= cm; w1 &= cm; }
+    const uint32_t top01 = nibble_counts(w0) + nibble_counts(w1);
     // Outer cells of group g: 4-column blocks g and g + 4 of those four rows (byte lanes as in
     // the boxes: even groups from even blocks, odd groups from odd blocks).
     const uint32_t E = (top01 & 0x0F0F0F0Fu) + (n23 & 0x0F0F0F0Fu);
@@ -210,31 +199,32 @@ __device__ __forceinline__ void second_test(BandSmem& S, uint32_t flag, uint32_t
     const uint32_t En = __shfl_down_sync(kFull, E, 1), On = __shfl_down_sync(kFull, O, 1);
     const uint32_t oe = E + __funnelshift_r(E, En, 16), oo = O + __funnelshift_r(O, On, 16);
     const uint32_t f2 = (bytes_at_least(re - oe, thr4) | (bytes_at_least(ro - oo, thr4) >> 1)) & flag;
-    if (f2) {
-        uint32_t gm = 0;  // bit 8j+7 -> group 2j, bit 8j+6 -> group 2j+1
-        for (uint32_t f = f2; f; f &= f - 1) {
-            const int bit = __ffs(f) - 1;
-            gm |= 1u << (2 * (bit >> 3) + 7 - (bit & 7));
-        }
-        const uint32_t left = push_groups(S, combo, lane, gm, st);
-        if (left) S.pend[t][combo][lane] = (uint8_t)left;
+    uint32_t gm = 0;  // bit 8j+7 -> group 2j, bit 8j+6 -> group 2j+1
+    for (uint32_t f = f2; f; f &= f - 1) {
+        const int bit = __ffs(f) - 1;
+        gm |= 1u << (2 * (bit >> 3) + 7 - (bit & 7));
+    }
+    for (unsigned todo = __ballot_sync(kFull, gm != 0); todo; todo &= todo - 1) {
+        const int word = __ffs(todo) - 1;
+        for (uint32_t gw = __shfl_sync(kFull, gm, word); gw; gw &= gw - 1)
+            exact_group<kMasked>(S, a, T, combo, fx, word, __ffs(gw) - 1, st, lane);
     }
 }
 
-// Counts one 4-row strip (rows 4t..4t+3 of ring[buf]) for the warp's four combo slots as one
-// straight-line block: 4x4 block counts, 20-column strip sums, rolling 20x20 boxes and the
+// Counts one 4-row strip (rows 4t..4t+3 of ring slot `slot`) for the warp's four combo slots as
+// one straight-line block: 4x4 block counts, 20-column strip sums, rolling 20x20 boxes and the
 // threshold test. Only when a lane flags a group does the warp take the second test. Slots of
 // combos beyond the launch's band count read zero planes and never flag.
 template <bool kMasked>
-__device__ __forceinline__ void count_strip(BandSmem& S, const BandArgs& a, Counter& C, int buf, int t,
-                                            int st, int warp, int lane, uint32_t fx, uint32_t lastmask,
-                                            uint32_t thr4, uint32_t& guard) {
+__device__ __forceinline__ void count_strip(BandSmem& S, const BandArgs& a, const Tile& T, Counter& C,
+                                            int slot, int t, int st, int warp, int lane, uint32_t fx,
+                                            uint32_t lastmask, uint32_t thr4, uint32_t& guard) {
     const int r0 = 4 * t;  // t is a compile-time constant after unrolling
     const int hs = st % 5;
     const uint32_t live = st >= 4 ? lastmask : 0u;  // boxes are complete from the fifth strip on
     uint32_t sel[4];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) sel[q] = S.ring[buf][r0 + q][kSwPlane][lane] ^ fx;
+    for (int q = 0; q < 4; ++q) sel[q] = S.ring[slot][r0 + q][kSwPlane][lane] ^ fx;
     uint32_t fl[kSlots], n23s[kSlots];
     uint32_t any = 0;
 #pragma unroll
@@ -244,7 +234,7 @@ __device__ __forceinline__ void count_strip(BandSmem& S, const BandArgs& a, Coun
         uint32_t n[4];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-            uint32_t w = S.ring[buf][r0 + q][m][lane] & sel[q];
+            uint32_t w = S.ring[slot][r0 + q][m][lane] & sel[q];
             if (kMasked) w &= C.cm[k];
             n[q] = nibble_counts(w);
         }
@@ -264,7 +254,6 @@ __device__ __forceinline__ void count_strip(BandSmem& S, const BandArgs& a, Coun
         C.ro[k] += go - *ho;
         *he = ge;
         *ho = go;
-        S.hist_n[hs][combo][lane] = n01;
         const uint32_t te = bytes_at_least(C.re[k], thr4), to = bytes_at_least(C.ro[k], thr4);
         fl[k] = (te | (to >> 1)) & live;  // even groups at bits 8j+7, odd groups at 8j+6
         n23s[k] = n23;
@@ -274,37 +263,8 @@ __device__ __forceinline__ void count_strip(BandSmem& S, const BandArgs& a, Coun
 #pragma unroll
         for (int k = 0; k < kSlots; ++k)
             if (__any_sync(kFull, fl[k] != 0))
-                second_test(S, fl[k], C.re[k], C.ro[k], n23s[k], thr4, warp + kWarps * k, lane, st, t);
-    }
-}
-
-// Processes the queue (all threads; block-uniform entry) and re-pushes pending groups of batch
-// `bprev`. With `final` it repeats until queue and pending groups are empty; otherwise it may
-// return with a partial queue (fewer than kQueueFlush groups) and no pending groups.
-__device__ __forceinline__ void drain_queue(BandSmem& S, const BandArgs& a, const Tile& T, int tid, int warp,
-                                            int lane, int bprev, bool final) {
-    for (;;) {
-        flush_queue(S, a, T, warp, lane);
-        const bool over = __syncthreads_or(S.qover != 0);
-        if (tid == 0) { S.qcount = 0; S.qover = 0; }
-        __syncthreads();
-        bool left = false;
-        if (over) {
-            for (int i = tid; i < 2 * kMaxCombos * kWords; i += kTpb) {
-                uint8_t* p = &S.pend[0][0][0] + i;
-                const uint32_t gm = *p;
-                if (gm) {
-                    const int t = i / (kMaxCombos * kWords), combo = (i / kWords) % kMaxCombos;
-                    const uint32_t rest = push_groups(S, combo, i % kWords, gm, 2 * bprev + t);
-                    *p = (uint8_t)rest;
-                    left |= rest != 0;
-                }
-            }
-        }
-        const bool more = __syncthreads_or(left);
-        const int queued = S.qcount;  // stable: every push precedes the barrier above
-        if (more) continue;
-        if (queued == 0 || (!final && queued < kQueueFlush)) break;
+                second_test<kMasked>(S, a, T, fl[k], C.re[k], C.ro[k], n23s[k], kMasked ? C.cm[k] : ~0u, fx,
+                                     thr4, warp + kWarps * k, lane, st);
     }
 }
 
@@ -320,16 +280,13 @@ __global__ void __launch_bounds__(kTpb, 1) band_scan_kernel(const BandArgs a) {
     uint32_t guard = 0;
     uint32_t bar_phase = 0;  // bit r: parity of the next completion of rows_bar[r]
     if (tid == 0) {
-        S.qcount = 0;
-        S.qover = 0;
         S.failed = 0;
         for (int r = 0; r < 3; ++r)
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&S.rows_bar[r])) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     // Planes of bands beyond nb are never generated: they stay zero and count nothing.
-    for (int i = tid; i < 2 * kBatchRows * kPlanes * kWords; i += kTpb) (&S.ring[0][0][0][0])[i] = 0;
-    for (int i = tid; i < 2 * kMaxCombos * kWords; i += kTpb) (&S.pend[0][0][0])[i] = 0;
+    for (int i = tid; i < kRingSlots * kBatchRows * kPlanes * kWords; i += kTpb) (&S.ring[0][0][0][0])[i] = 0;
     // Counter constants: the swap sense of the warp's phase and the groups lane 31 may flag
     // (groups 4..7 of word 31 hold centres 1,008+ of the tile, which belong to the next tile).
     const uint32_t fx = ((warp ^ (warp >> 1)) & 1) ? 0u : ~0u;
@@ -366,15 +323,11 @@ __global__ void __launch_bounds__(kTpb, 1) band_scan_kernel(const BandArgs a) {
             xh0[k] = (uint32_t)(x0 >> kPeriodBits);
             xh1[k] = (uint32_t)(x1 >> kPeriodBits);
         }
-        // Counter slots of this warp: combo rows warp + 16*k; lane = word. Columns of the word
-        // that exist for the slot's phase (bits beyond are masked to zero before counting).
+        // Counter slots of this warp: combo rows warp + 16*k; lane = word.
         Counter C;
 #pragma unroll
         for (int k = 0; k < kSlots; ++k) {
-            const int combo = warp + kWarps * k;
-            const int64_t first = (int64_t)T.u0 + lane * 32 + (int64_t)(T.i0 + (combo & 1)) * kPeriod;
-            const int64_t nvalid = a.ncols - first;
-            C.cm[k] = nvalid >= 32 ? ~0u : nvalid <= 0 ? 0u : (1u << nvalid) - 1u;
+            C.cm[k] = column_mask(a, T, lane, (warp + kWarps * k) & 1);
             C.re[k] = C.ro[k] = 0;
         }
         // Tiles whose columns all exist in both phases skip the column masks (block-uniform).
@@ -383,7 +336,6 @@ __global__ void __launch_bounds__(kTpb, 1) band_scan_kernel(const BandArgs a) {
         for (int i = tid; i < 5 * kMaxCombos * kWords; i += kTpb) {
             (&S.hist_e[0][0][0])[i] = 0;
             (&S.hist_o[0][0][0])[i] = 0;
-            (&S.hist_n[0][0][0])[i] = 0;
         }
         // Row terms of batches 0 and 1 (batch b lives in rows[b % 3]).
         if (tid == 0) {
@@ -394,8 +346,8 @@ __global__ void __launch_bounds__(kTpb, 1) band_scan_kernel(const BandArgs a) {
         __syncthreads();
 
         for (int b = 0; b < batches; ++b) {
-            const int rb = b % 3, buf = b & 1;
-            // ---- generator: batch b into ring[buf] ------------------------------------------
+            const int rb = b % 3, slot = b & (kRingSlots - 1);
+            // ---- generator: batch b into ring slot b % 4 ------------------------------------
             if (!bar_wait(&S.rows_bar[rb], (bar_phase >> rb) & 1u)) {
                 S.failed = 1;
                 if (lane == 0) atomicOr(a.overflow, 4u);
@@ -422,7 +374,7 @@ __global__ void __launch_bounds__(kTpb, 1) band_scan_kernel(const BandArgs a) {
                 }
                 // Plane m of the warp's 4 words at dst + m * kWords (16-byte aligned). Every lane
                 // stores the same ballot words to the same address: no predicate, no branch.
-                uint4* dst = reinterpret_cast<uint4*>(&S.ring[buf][q][0][gw]);
+                uint4* dst = reinterpret_cast<uint4*>(&S.ring[slot][q][0][gw]);
                 constexpr int kPlaneStep = kWords / 4;  // uint4 per plane
                 dst[kSwPlane * kPlaneStep] = make_uint4(sw[0], sw[1], sw[2], sw[3]);
                 auto hit = [&](uint32_t x, uint32_t z, uint32_t d) {
@@ -461,25 +413,21 @@ __global__ void __launch_bounds__(kTpb, 1) band_scan_kernel(const BandArgs a) {
             __syncthreads();
             if (S.failed) return;  // block-uniform after the barrier
 
-            // ---- survivor queue: flush when half full; groups that did not fit are re-pushed ---
-            if (S.qcount >= kQueueFlush || S.qover)
-                drain_queue(S, a, T, tid, warp, lane, b - 1, false);
             // Row terms of batch b + 2 (its buffer was last read before this batch's barrier).
             if (tid == kTpb - 32 && b + 2 < batches)
                 bulk_load(&S.rows[(b + 2) % 3][0][0], a.rt + (int64_t)(T.v0 + kBatchRows * (b + 2)) * kRowWords,
                           kBatchBytes, &S.rows_bar[(b + 2) % 3]);
 
-            // ---- counter: the two strips of batch b from ring[buf] ---------------------------
+            // ---- counter: the two strips of batch b ------------------------------------------
 #pragma unroll
             for (int t = 0; t < 2; ++t) {
                 if (interior)
-                    count_strip<false>(S, a, C, buf, t, 2 * b + t, warp, lane, fx, lastmask, thr4, guard);
+                    count_strip<false>(S, a, T, C, slot, t, 2 * b + t, warp, lane, fx, lastmask, thr4, guard);
                 else
-                    count_strip<true>(S, a, C, buf, t, 2 * b + t, warp, lane, fx, lastmask, thr4, guard);
+                    count_strip<true>(S, a, T, C, slot, t, 2 * b + t, warp, lane, fx, lastmask, thr4, guard);
             }
         }
-        __syncthreads();
-        drain_queue(S, a, T, tid, warp, lane, batches - 1, true);
+        __syncthreads();  // the next tile reuses ring slots and histories still read above
     }
     // A 4-row strip with 52+ hits among its 80 cells could carry a box past a byte lane.
     if (guard & 0x80808080u) atomicOr(a.overflow, 1u);
