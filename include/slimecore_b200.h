@@ -118,10 +118,12 @@ void slime_b200_last_search_stats(double* kernel_ms, int64_t* launches);
  * that used the band engine; 0 otherwise. */
 int64_t slime_b200_last_rare_chunks(void);
 
-/* Engine selection: mode 0 automatic, 1 always the general scan, 2 the band engine whenever the
- * threshold allows it (min_size >= 28). `band_min_threshold` (28..221, other values keep the
- * current one) is the smallest threshold automatic mode sends to the band engine. Results are
- * identical either way; only speed differs. */
+/* Engine selection: mode 0 automatic, 1 always the general scan, 2 the shared-LCG band engine
+ * and 3 the independent-band engine whenever the threshold allows it (min_size >= 28).
+ * `band_min_threshold` (28..221, other values keep the current one) is the smallest threshold
+ * automatic mode sends to the shared-LCG band engine. Results are identical either way; only
+ * speed differs. get_gpu_v1_algorithm() reports 100 (general), 200 (band) or 300 (independent
+ * bands) for the last search. */
 void slime_b200_set_engine(int32_t mode, int32_t band_min_threshold);
 
 /* Generator variant of the band engine (results are identical): band_mad_add != 0 issues the

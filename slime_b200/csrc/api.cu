@@ -346,10 +346,11 @@ int64_t Context::search(const SearchSpec& q, ExtChunkResult* results) {
     std::vector<uint32_t> h(kHistBins, 0u);
     bool cancelled = false;
     last_rare = 0;
-    const bool band = band_eligible(q);
-    last_algorithm = band ? kAlgoBand : kAlgoGeneral;
-    last_shape = band ? 3 : (2 * q.rd_max + 1) < 8192 ? 1 : 2;
-    if (!(band ? scan_band(q, best, h, cancelled) : scan_general(q, best, h, cancelled))) {
+    const int32_t algo = engine_for(q);
+    last_algorithm = algo;
+    last_shape = algo == kAlgoBand ? 3 : algo == kAlgoIndep ? 4 : (2 * q.rd_max + 1) < 8192 ? 1 : 2;
+    if (!(algo == kAlgoGeneral ? scan_general(q, best, h, cancelled)
+                               : scan_band(q, best, h, cancelled, algo == kAlgoIndep))) {
         progress.store(0);
         return -1;
     }
@@ -534,7 +535,7 @@ void slime_b200_set_tuning(int32_t band_mad_add) {
 
 void slime_b200_set_engine(int32_t mode, int32_t band_min_threshold) {
     std::lock_guard<std::mutex> lock(ctx().mu);
-    ctx().engine_override = (mode >= 0 && mode <= 2) ? mode : 0;
+    ctx().engine_override = (mode >= 0 && mode <= 3) ? mode : 0;
     if (band_min_threshold >= 28 && band_min_threshold <= 221) ctx().band_min_threshold = band_min_threshold;
 }
 

@@ -34,33 +34,49 @@ bool Context::ensure_band() {
     return true;
 }
 
-// The band engine needs a threshold >= 28 (its byte-lane bound test); automatic selection also
-// wants an area spanning two periods on one axis and a threshold high enough for its bound.
-bool Context::band_eligible(const SearchSpec& q) const {
-    if (q.min_size < 28 || engine_override == 1) return false;
-    if (engine_override == 2) return true;
+// Engine choice. The band engines need a threshold >= 28 (their byte-lane bound test). The
+// shared-LCG band engine wants an area spanning two periods on one axis; the independent-band
+// engine wants enough centres to fill the GPU. Below their thresholds the exact counts of the
+// many surviving 4x4 groups dominate and the general scan is faster.
+int32_t Context::engine_for(const SearchSpec& q) const {
+    if (engine_override == 1 || q.min_size < 28) return kAlgoGeneral;
+    if (engine_override == 2) return kAlgoBand;
+    if (engine_override == 3) return kAlgoIndep;
+    // Measured on B200 (T centres/s, shared band / independent bands): radius 300k thr 50
+    // 0.76 / 1.00, thr 60 1.84 / -; radius 600k thr 50 1.06 / 1.02, thr 60 3.27 / 1.52. The shared
+    // LCG pays off with many periods or a high threshold.
     const int64_t w = 2 * q.rd_max + 1;
-    return w >= 2 * kP && q.min_size >= band_min_threshold;
+    if (w >= 2 * kP && q.min_size >= band_min_threshold &&
+        (q.min_size >= 55 || w >= 8 * kP))
+        return kAlgoBand;
+    if (w * w >= indep_min_centres && q.min_size >= indep_min_threshold) return kAlgoIndep;
+    return kAlgoGeneral;
 }
 
 bool Context::scan_band(const SearchSpec& q, std::vector<Hit>& best, std::vector<uint32_t>& h,
-                        bool& cancelled) {
+                        bool& cancelled, bool indep) {
     if (!ensure_band()) return false;
     const int64_t W = 2 * q.rd_max + 1, H = W;
     const int32_t area_x0 = (int32_t)((int64_t)q.center_x - q.rd_max);
     const int32_t area_z0 = (int32_t)((int64_t)q.center_z - q.rd_max);
-    const bool transposed = W < 2 * kP && H >= 2 * kP;
+    const bool transposed = !indep && W < 2 * kP && H >= 2 * kP;
     const int64_t width_u = transposed ? H : W, height_v = transposed ? W : H;
-    const int64_t nI = (width_u + kP - 1) / kP, nJ = (height_v + kP - 1) / kP;
-    const int32_t ubase = (int32_t)std::min(kP, width_u), vbase = (int32_t)std::min(kP, height_v);
+    const int out_w = band_tile_out_w();
+    const int nb_max = band_max_bands();
+    // Shared LCG: X phases and Z bands 2^17 apart. Independent bands: one phase, nJ bands of
+    // `stride` rows each (at least 256 rows a band, at most 32 bands).
+    const int64_t nI = indep ? 1 : (width_u + kP - 1) / kP;
+    const int64_t nJ = indep ? std::max<int64_t>(1, std::min<int64_t>(nb_max, height_v / 256))
+                             : (height_v + kP - 1) / kP;
+    const int64_t stride = indep ? (height_v + nJ - 1) / nJ : kP;
+    const int32_t ubase = (int32_t)(indep ? width_u : std::min(kP, width_u));
+    const int32_t vbase = (int32_t)std::min(stride, height_v);
     const int32_t vrows = vbase + 16;
     const int32_t vrows_alloc = vbase + 32;  // zero rows: 8-row bulk copies never run past the end
-    const int nb_max = band_max_bands();
     const int64_t ngroups = (nJ + nb_max - 1) / nb_max;
-    const int out_w = band_tile_out_w();
     cudaError_t e;
     if ((e = xt.reserve((size_t)width_u + 16)) != cudaSuccess ||
-        (e = rt.reserve((size_t)ngroups * vrows_alloc * band_row_words())) != cudaSuccess ||
+        (e = rt.reserve((size_t)ngroups * vrows_alloc * band_row_words(indep))) != cudaSuccess ||
         (e = counters.reserve(4)) != cudaSuccess ||
         (e = hits.reserve(hit_capacity(q.max_results))) != cudaSuccess ||
         (e = fixed.reserve(1u << 20)) != cudaSuccess) {
@@ -70,7 +86,8 @@ bool Context::scan_band(const SearchSpec& q, std::vector<Hit>& best, std::vector
     const int32_t col_first = (transposed ? area_z0 : area_x0) - 8;
     const int32_t row_first = (transposed ? area_x0 : area_z0) - 8;
     if ((e = launch_band_terms(xt.ptr, col_first, (int32_t)(width_u + 16), rt.ptr, vrows_alloc, vrows,
-                               (int32_t)nJ, row_first, height_v + 16, q.seed, transposed, stream)) != cudaSuccess) {
+                               (int32_t)nJ, row_first, height_v + 16, stride, q.seed, transposed, indep,
+                               stream)) != cudaSuccess) {
         set_error("band terms", e);
         return false;
     }
@@ -91,8 +108,16 @@ bool Context::scan_band(const SearchSpec& q, std::vector<Hit>& best, std::vector
     if (nrare > kRareCap) { set_error("too many rare chunks", cudaErrorMemoryAllocation); return false; }
     last_rare = nrare;
 
-    const int32_t band_h = (int32_t)std::min<int64_t>(2048, std::max<int64_t>(256, vbase));
-    const int64_t u_tiles = (ubase + out_w - 1) / out_w, v_tiles = (vbase + band_h - 1) / band_h;
+    const int64_t u_tiles = (ubase + out_w - 1) / out_w;
+    int32_t band_h = (int32_t)std::min<int64_t>(2048, std::max<int64_t>(256, vbase));
+    if (indep) {
+        // Enough tiles for two waves of CTAs where the area allows it, tiles of 64+ rows.
+        const int64_t want = (2 * (int64_t)sm_count + u_tiles - 1) / u_tiles;
+        const int64_t vt = std::max<int64_t>((vbase + 2047) / 2048,
+                                             std::min<int64_t>((vbase + 63) / 64, want));
+        band_h = (int32_t)((vbase + vt - 1) / vt);
+    }
+    const int64_t v_tiles = (vbase + band_h - 1) / band_h;
     const int64_t pairs = (nI + 1) / 2;
     const int grid = sm_count;
     const uint64_t cap = hits.count;
@@ -110,7 +135,7 @@ bool Context::scan_band(const SearchSpec& q, std::vector<Hit>& best, std::vector
             BandArgs a{};
             a.ct = xt.ptr;
             a.ncols = width_u + 16;
-            a.rt = rt.ptr + (size_t)g * vrows_alloc * band_row_words();
+            a.rt = rt.ptr + (size_t)g * vrows_alloc * band_row_words(indep);
             a.vrows = vrows;
             a.vbase = vbase;
             a.ubase = ubase;
@@ -137,6 +162,8 @@ bool Context::scan_band(const SearchSpec& q, std::vector<Hit>& best, std::vector
             a.overflow = flags.ptr;
             a.one = 1u;
             a.mad_add = band_mad_add;
+            a.indep = indep ? 1 : 0;
+            a.row_stride = stride;
             const auto c0 = std::chrono::steady_clock::now();
             if ((e = cudaMemsetAsync(counters.ptr, 0, 8, stream)) != cudaSuccess ||
                 (e = cudaEventRecord(ev_a, stream)) != cudaSuccess ||

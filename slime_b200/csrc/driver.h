@@ -51,6 +51,7 @@ struct SearchSpec {
 // Values reported by get_gpu_v1_algorithm().
 constexpr int32_t kAlgoGeneral = 100;
 constexpr int32_t kAlgoBand = 200;
+constexpr int32_t kAlgoIndep = 300;
 
 constexpr size_t kPinnedBytes = 1 << 20;
 
@@ -96,11 +97,15 @@ struct Context {
     DeviceBuffer<Hit> fixed;
     DeviceBuffer<unsigned int> flags;  // [0] overflow, [1] fix-up error, [2] rare count
     bool band_ready = false;
-    int32_t engine_override = 0;       // 0 auto, 1 general scan, 2 band engine
-    // Auto mode uses the band engine from this threshold: below it the exact counts of the many
-    // surviving 4x4 groups dominate and the general scan is faster (B200 crossover measured
+    int32_t engine_override = 0;       // 0 auto, 1 general scan, 2 band engine, 3 independent bands
+    // Auto mode uses the shared-LCG band engine from this threshold: below it the exact counts of
+    // the many surviving 4x4 groups dominate (B200 crossover with the general scan measured
     // between 45 and 48 on a 1,200,001^2 area).
-    int32_t band_min_threshold = 47;
+    int32_t band_min_threshold = 48;
+    // Auto mode uses the independent-band engine for areas of at least this many centres from
+    // this threshold on.
+    int32_t indep_min_threshold = 44;
+    int64_t indep_min_centres = 1000000000;
     int64_t last_rare = 0;             // rare redraw chunks found by the last band search
     int64_t band_fallbacks = 0;        // band searches redone by the general scan
     int32_t band_mad_add = 1;          // generator variant: band adds on the multiply pipe
@@ -133,9 +138,9 @@ struct Context {
     bool scan_general(const SearchSpec& q, std::vector<Hit>& best, std::vector<uint32_t>& hist_out,
                       bool& cancelled);
     bool ensure_band();
-    bool band_eligible(const SearchSpec& q) const;
+    int32_t engine_for(const SearchSpec& q) const;
     bool scan_band(const SearchSpec& q, std::vector<Hit>& best, std::vector<uint32_t>& hist_out,
-                   bool& cancelled);
+                   bool& cancelled, bool indep);
     bool score(int64_t seed, ExtChunkResult* host, int32_t n, int32_t scan_xz, bool pack);
     int64_t search(const SearchSpec& q, ExtChunkResult* results);
 };

@@ -87,6 +87,8 @@ struct BandArgs {
     unsigned int* overflow;
     uint32_t one;            // the value 1 (run time): band adds as multiply-adds when mad_add
     int32_t mad_add;
+    int32_t indep;           // 1: independent bands (no shared LCG work, one X phase)
+    int64_t row_stride;      // input rows between band j and band j + 1 (2^17 with the shared LCG)
 };
 
 size_t band_smem_bytes();
@@ -94,10 +96,11 @@ int band_tile_out_w();
 int band_max_bands();
 cudaError_t band_prepare();
 cudaError_t launch_band_scan(const BandArgs& a, int grid, cudaStream_t s);
-int band_row_words();
+int band_row_words(bool indep);
 cudaError_t launch_band_terms(uint64_t* ct, int32_t col_first, int32_t ncols, uint32_t* rt,
                               int32_t vrows_alloc, int32_t vrows, int32_t nj, int32_t row_first,
-                              int64_t row_limit, int64_t seed, bool transposed, cudaStream_t s);
+                              int64_t row_limit, int64_t row_stride, int64_t seed, bool transposed,
+                              bool indep, cudaStream_t s);
 
 // ---- rare redraw correction (rare_fix.cu) ------------------------------------------------
 

@@ -45,6 +45,14 @@ constexpr int kRowWords = 36;
 constexpr int kRowLo = 32;      // low 17 bits of the row term (shared by all bands)
 constexpr int kRowValid = 33;   // bands of the group that hold this row (prefix count)
 
+// Independent-band record (general mode: bands at any row spacing, no shared low bits):
+// [m] high part and [32 + m] low 17 bits of the row term in band m, [64] bands holding the row.
+constexpr int kRowWordsI = 72;
+constexpr int kRowLoI = 32;
+constexpr int kRowValidI = 64;
+template <bool kIndep>
+constexpr int row_words() { return kIndep ? kRowWordsI : kRowWords; }
+
 constexpr int kBatchRows = 8;               // rows per barrier: two 4-row strips
 constexpr int kRingSlots = 4;               // batches b-2..b are read while b+1 is generated
 
@@ -52,7 +60,7 @@ struct __align__(16) BandSmem {
     uint32_t ring[kRingSlots][kBatchRows][kPlanes][kWords];  // [batch % 4][row][band planes | swap][word]
     uint32_t hist_e[5][kMaxCombos][kWords];   // strip sums of the last 5 strips (even groups)
     uint32_t hist_o[5][kMaxCombos][kWords];   // (odd groups)
-    uint32_t rows[3][kBatchRows][kRowWords];  // row terms of 3 batches, filled by bulk copies
+    uint32_t rows[3][kBatchRows * kRowWordsI];  // row terms of 3 batches, filled by bulk copies
     unsigned long long rows_bar[3];           // mbarriers of the three row-term buffers
     int failed;  // a bounded wait gave up: the CTA stops
 };
@@ -108,26 +116,35 @@ __device__ __forceinline__ uint32_t column_mask(const BandArgs& a, const Tile& T
     return nvalid >= 32 ? ~0u : nvalid <= 0 ? 0u : (1u << nvalid) - 1u;
 }
 
-// Bits of combo (ph, m) in ring row `r` (tile-relative input row), word `word`.
-__device__ __forceinline__ uint32_t combo_word(const BandSmem& S, int r, int m, uint32_t fx, int word) {
+// A combo is one (X phase, band) pair: combo = 2 m + phase with the shared LCG, combo = m for
+// independent bands (one phase).
+template <bool kIndep>
+__device__ __forceinline__ int combo_band(int combo) { return kIndep ? combo : combo >> 1; }
+template <bool kIndep>
+__device__ __forceinline__ int combo_phase(int combo) { return kIndep ? 0 : combo & 1; }
+
+// Bits of a combo in ring row `r` (tile-relative input row), word `word`.
+template <bool kIndep>
+__device__ __forceinline__ uint32_t combo_word(const BandSmem& S, int r, int combo, uint32_t fx, int word) {
     const int slot = (r >> 3) & (kRingSlots - 1), q = r & 7;
-    return S.ring[slot][q][m][word] & (S.ring[slot][q][kSwPlane][word] ^ fx);
+    if (kIndep) return S.ring[slot][q][combo][word];
+    return S.ring[slot][q][combo >> 1][word] & (S.ring[slot][q][kSwPlane][word] ^ fx);
 }
 
 // Exact window counts of the 16 centres of group g of word `word` for one combo, from the 20
 // ring rows of strips st-4..st. Lanes 0..19 fetch one 20-column row slice each; lanes 0..15 then
 // count one centre (dx = lane & 3, dz = lane >> 2) over 17 shuffled slices. Centres in range are
 // appended to the hit list. Warp-uniform arguments; called by the whole warp.
-template <bool kMasked>
+template <bool kMasked, bool kIndep>
 __device__ __forceinline__ void exact_group(const BandSmem& S, const BandArgs& a, const Tile& T, int combo,
                                          uint32_t fx, int word, int g, int st, int lane) {
-    const int ph = combo & 1, m = combo >> 1;
+    const int ph = combo_phase<kIndep>(combo), m = combo_band<kIndep>(combo);
     const int c0 = word * 32 + 4 * g;       // first window column (tile-relative input col)
     const int r0 = 4 * (st - 4);            // first window row (tile-relative input row)
     uint32_t slice = 0;
     if (lane < 20) {
-        uint32_t lo = combo_word(S, r0 + lane, m, fx, word);
-        uint32_t hi = word + 1 < kWords ? combo_word(S, r0 + lane, m, fx, word + 1) : 0u;
+        uint32_t lo = combo_word<kIndep>(S, r0 + lane, combo, fx, word);
+        uint32_t hi = word + 1 < kWords ? combo_word<kIndep>(S, r0 + lane, combo, fx, word + 1) : 0u;
         if (kMasked) {
             lo &= column_mask(a, T, word, ph);
             hi &= word + 1 < kWords ? column_mask(a, T, word + 1, ph) : 0u;
@@ -147,7 +164,7 @@ __device__ __forceinline__ void exact_group(const BandSmem& S, const BandArgs& a
         const int c = c0 + dx, rr = r0 + dz;
         const int64_t u = (int64_t)T.u0 + c, v = (int64_t)T.v0 + rr;
         const int64_t cu = u + (int64_t)(T.i0 + ph) * kPeriod;
-        const int64_t cv = v + (int64_t)(a.j0 + m) * kPeriod;
+        const int64_t cv = v + (int64_t)(a.j0 + m) * a.row_stride;
         keep = count >= a.min_size && count <= a.max_size && c < kOutW && u < a.ubase &&
                rr < T.out_h && cu < a.width_u && cv < a.height_v;
         if (keep) {
@@ -182,13 +199,12 @@ struct Counter {
 // outer cells of rows 0, 1 (strip st - 4) and of rows 18, 19 (strip st), which no window of the
 // group reaches, are removed from the box (368 cells remain; the box bytes are exact, so no byte
 // borrows). Survivors are counted exactly. Called by the whole warp.
-template <bool kMasked>
+template <bool kMasked, bool kIndep>
 __device__ __forceinline__ void second_test(const BandSmem& S, const BandArgs& a, const Tile& T, uint32_t flag,
                                             uint32_t re, uint32_t ro, uint32_t n23, uint32_t cm, uint32_t fx,
                                             uint32_t thr4, int combo, int lane, int st) {
-    const int m = combo >> 1;
     const int r0 = 4 * (st - 4);  // rows 0 and 1 of strip st - 4
-    uint32_t w0 = combo_word(S, r0, m, fx, lane), w1 = combo_word(S, r0 + 1, m, fx, lane);
+    uint32_t w0 = combo_word<kIndep>(S, r0, combo, fx, lane), w1 = combo_word<kIndep>(S, r0 + 1, combo, fx, lane);
     if (kMasked) { w0 &= cm; w1 &= cm; }
     const uint32_t top01 = nibble_counts(w0) + nibble_counts(w1);
     // Outer cells of group g: 4-column blocks g and g + 4 of those four rows (byte lanes as in
@@ -207,30 +223,33 @@ __device__ __forceinline__ void second_test(const BandSmem& S, const BandArgs& a
     for (unsigned todo = __ballot_sync(kFull, gm != 0); todo; todo &= todo - 1) {
         const int word = __ffs(todo) - 1;
         for (uint32_t gw = __shfl_sync(kFull, gm, word); gw; gw &= gw - 1)
-            exact_group<kMasked>(S, a, T, combo, fx, word, __ffs(gw) - 1, st, lane);
+            exact_group<kMasked, kIndep>(S, a, T, combo, fx, word, __ffs(gw) - 1, st, lane);
     }
 }
 
 // Counts one 4-row strip (rows 4t..4t+3 of ring slot `slot`) for the warp's four combo slots as
 // one straight-line block: 4x4 block counts, 20-column strip sums, rolling 20x20 boxes and the
-// threshold test. Only when a lane flags a group does the warp take the second test. Slots of
-// combos beyond the launch's band count read zero planes and never flag.
-template <bool kMasked>
+// threshold test. Only when a lane flags a group does the warp take the second test. With the
+// shared LCG, slots of combos beyond the launch's band count read zero planes and never flag;
+// independent bands use two slots per warp (32 combos) and skip combos beyond the band count.
+template <bool kMasked, bool kIndep>
 __device__ __forceinline__ void count_strip(BandSmem& S, const BandArgs& a, const Tile& T, Counter& C,
                                             int slot, int t, int st, int warp, int lane, uint32_t fx,
                                             uint32_t lastmask, uint32_t thr4, uint32_t& guard) {
     const int r0 = 4 * t;  // t is a compile-time constant after unrolling
     const int hs = st % 5;
     const uint32_t live = st >= 4 ? lastmask : 0u;  // boxes are complete from the fifth strip on
+    constexpr int kUsed = kIndep ? kMaxBands / kWarps : kSlots;
     uint32_t sel[4];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) sel[q] = S.ring[slot][r0 + q][kSwPlane][lane] ^ fx;
-    uint32_t fl[kSlots], n23s[kSlots];
+    for (int q = 0; q < 4; ++q) sel[q] = kIndep ? ~0u : S.ring[slot][r0 + q][kSwPlane][lane] ^ fx;
+    uint32_t fl[kSlots] = {}, n23s[kSlots] = {};
     uint32_t any = 0;
 #pragma unroll
-    for (int k = 0; k < kSlots; ++k) {
+    for (int k = 0; k < kUsed; ++k) {
         const int combo = warp + kWarps * k;
-        const int m = combo >> 1;
+        const int m = combo_band<kIndep>(combo);
+        if (kIndep && m >= a.nb) continue;  // warp-uniform
         uint32_t n[4];
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
@@ -261,14 +280,26 @@ __device__ __forceinline__ void count_strip(BandSmem& S, const BandArgs& a, cons
     }
     if (__any_sync(kFull, any != 0)) {
 #pragma unroll
-        for (int k = 0; k < kSlots; ++k)
+        for (int k = 0; k < kUsed; ++k)
             if (__any_sync(kFull, fl[k] != 0))
-                second_test<kMasked>(S, a, T, fl[k], C.re[k], C.ro[k], n23s[k], kMasked ? C.cm[k] : ~0u, fx,
-                                     thr4, warp + kWarps * k, lane, st);
+                second_test<kMasked, kIndep>(S, a, T, fl[k], C.re[k], C.ro[k], n23s[k], kMasked ? C.cm[k] : ~0u,
+                                             fx, thr4, warp + kWarps * k, lane, st);
     }
 }
 
+// First-draw test of one chunk from split terms (independent bands: nothing is shared).
 template <bool kMadAdd>
+__device__ __forceinline__ bool indep_hit(uint32_t xl, uint32_t xh, uint32_t zl, uint32_t zh, uint32_t one) {
+    const uint32_t s = kMadAdd ? xl * one + zl : xl + zl;
+    const uint32_t l = (s & 0x1FFFFu) ^ kXorLo;
+    const uint64_t prod = (uint64_t)l * kA32 + 11u;
+    const uint32_t q = (uint32_t)(prod >> kPeriodBits) + l * kQLimbMul;
+    const uint32_t h = (xh + zh + (s >> kPeriodBits)) ^ kXorHi;
+    const uint32_t t = h * kA32 + q;  // bits (mod 2^32): even and t * 2/5 small <=> slime
+    return !(t & 1u) && t * kTwoInv5 < kHitBelow;
+}
+
+template <bool kMadAdd, bool kIndep>
 __global__ void __launch_bounds__(kTpb, 1) band_scan_kernel(const BandArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     BandSmem& S = *reinterpret_cast<BandSmem*>(smem_raw);
@@ -298,17 +329,18 @@ __global__ void __launch_bounds__(kTpb, 1) band_scan_kernel(const BandArgs a) {
         const int ut = (int)(tile % a.u_tiles);
         const int64_t rest = tile / a.u_tiles;
         const int vt = (int)(rest % a.v_tiles);
-        T.i0 = 2 * (int)(rest / a.v_tiles);
+        T.i0 = kIndep ? 0 : 2 * (int)(rest / a.v_tiles);
         T.u0 = ut * kOutW;
         T.v0 = vt * a.band_h;
         // Tiles with no centre of the area in any of their combos are skipped (block-uniform).
         if ((int64_t)T.u0 + (int64_t)T.i0 * kPeriod >= a.width_u ||
-            (int64_t)T.v0 + (int64_t)a.j0 * kPeriod >= a.height_v)
+            (int64_t)T.v0 + (int64_t)a.j0 * a.row_stride >= a.height_v)
             continue;
         T.out_h = min(a.band_h, a.vbase - T.v0);
         const int strips = (T.out_h + 16 + 3) / 4;
         const int batches = (strips + 1) / 2;
-        constexpr uint32_t kBatchBytes = kBatchRows * kRowWords * 4;
+        constexpr int kRW = row_words<kIndep>();
+        constexpr uint32_t kBatchBytes = kBatchRows * kRW * 4;
 
         // Generator columns of this thread: words 4*(warp%8) .. +3, lane = bit; the warp
         // generates rows 4*(warp/8) .. +3 of every 8-row batch.
@@ -327,21 +359,21 @@ __global__ void __launch_bounds__(kTpb, 1) band_scan_kernel(const BandArgs a) {
         Counter C;
 #pragma unroll
         for (int k = 0; k < kSlots; ++k) {
-            C.cm[k] = column_mask(a, T, lane, (warp + kWarps * k) & 1);
+            C.cm[k] = column_mask(a, T, lane, combo_phase<kIndep>(warp + kWarps * k));
             C.re[k] = C.ro[k] = 0;
         }
         // Tiles whose columns all exist in both phases skip the column masks (block-uniform).
         // Rows need no mask: the generator writes zero words for bands that do not hold a row.
-        const bool interior = (int64_t)T.u0 + kWords * 32 + (int64_t)(T.i0 + 1) * kPeriod <= a.ncols;
+        const bool interior = (int64_t)T.u0 + kWords * 32 + (int64_t)(T.i0 + (kIndep ? 0 : 1)) * kPeriod <= a.ncols;
         for (int i = tid; i < 5 * kMaxCombos * kWords; i += kTpb) {
             (&S.hist_e[0][0][0])[i] = 0;
             (&S.hist_o[0][0][0])[i] = 0;
         }
         // Row terms of batches 0 and 1 (batch b lives in rows[b % 3]).
         if (tid == 0) {
-            bulk_load(&S.rows[0][0][0], a.rt + (int64_t)T.v0 * kRowWords, kBatchBytes, &S.rows_bar[0]);
+            bulk_load(&S.rows[0][0], a.rt + (int64_t)T.v0 * kRW, kBatchBytes, &S.rows_bar[0]);
             if (batches > 1)
-                bulk_load(&S.rows[1][0][0], a.rt + (int64_t)(T.v0 + kBatchRows) * kRowWords, kBatchBytes, &S.rows_bar[1]);
+                bulk_load(&S.rows[1][0], a.rt + (int64_t)(T.v0 + kBatchRows) * kRW, kBatchBytes, &S.rows_bar[1]);
         }
         __syncthreads();
 
@@ -353,10 +385,42 @@ __global__ void __launch_bounds__(kTpb, 1) band_scan_kernel(const BandArgs a) {
                 if (lane == 0) atomicOr(a.overflow, 4u);
             }
             bar_phase ^= 1u << rb;
+            if constexpr (kIndep) {
 #pragma unroll 1
             for (int qq = 0; qq < 4; ++qq) {
                 const int q = gq + qq;
-                const uint32_t* zr = &S.rows[rb][q][0];
+                const uint32_t* zr = &S.rows[rb][q * kRowWordsI];
+                const int nv = __shfl_sync(kFull, min((int)zr[kRowValidI], nb), 0);  // warp-uniform
+                uint4* dst = reinterpret_cast<uint4*>(&S.ring[slot][q][0][gw]);
+                constexpr int kPlaneStep = kWords / 4;
+                int m = 0;
+                for (; m + 1 < nv; m += 2) {
+                    const uint2 zh = *reinterpret_cast<const uint2*>(zr + m);
+                    const uint2 zl = *reinterpret_cast<const uint2*>(zr + kRowLoI + m);
+                    uint32_t wa[4], wb[4];
+#pragma unroll
+                    for (int k = 0; k < 4; ++k) {
+                        wa[k] = __ballot_sync(kFull, indep_hit<kMadAdd>(lox[k], xh0[k], zl.x, zh.x, one));
+                        wb[k] = __ballot_sync(kFull, indep_hit<kMadAdd>(lox[k], xh0[k], zl.y, zh.y, one));
+                    }
+                    dst[m * kPlaneStep] = make_uint4(wa[0], wa[1], wa[2], wa[3]);
+                    dst[(m + 1) * kPlaneStep] = make_uint4(wb[0], wb[1], wb[2], wb[3]);
+                }
+                if (m < nv) {
+                    uint32_t wa[4];
+#pragma unroll
+                    for (int k = 0; k < 4; ++k)
+                        wa[k] = __ballot_sync(kFull, indep_hit<kMadAdd>(lox[k], xh0[k], zr[kRowLoI + m], zr[m], one));
+                    dst[m * kPlaneStep] = make_uint4(wa[0], wa[1], wa[2], wa[3]);
+                    ++m;
+                }
+                for (; m < nb; ++m) dst[m * kPlaneStep] = make_uint4(0u, 0u, 0u, 0u);  // rows outside band m
+            }
+            } else {
+#pragma unroll 1
+            for (int qq = 0; qq < 4; ++qq) {
+                const int q = gq + qq;
+                const uint32_t* zr = &S.rows[rb][q * kRowWords];
                 const uint32_t zlo = zr[kRowLo];
                 // Bands 0..nv-1 hold this row. The broadcast tells the compiler that the value
                 // (and the loops it bounds) is warp-uniform.
@@ -410,21 +474,22 @@ __global__ void __launch_bounds__(kTpb, 1) band_scan_kernel(const BandArgs a) {
                     for (int m = nv; m < nb; ++m) dst[m * kPlaneStep] = make_uint4(0u, 0u, 0u, 0u);  // rows outside band m
                 }
             }
+            }
             __syncthreads();
             if (S.failed) return;  // block-uniform after the barrier
 
             // Row terms of batch b + 2 (its buffer was last read before this batch's barrier).
             if (tid == kTpb - 32 && b + 2 < batches)
-                bulk_load(&S.rows[(b + 2) % 3][0][0], a.rt + (int64_t)(T.v0 + kBatchRows * (b + 2)) * kRowWords,
+                bulk_load(&S.rows[(b + 2) % 3][0], a.rt + (int64_t)(T.v0 + kBatchRows * (b + 2)) * kRW,
                           kBatchBytes, &S.rows_bar[(b + 2) % 3]);
 
             // ---- counter: the two strips of batch b ------------------------------------------
 #pragma unroll
             for (int t = 0; t < 2; ++t) {
                 if (interior)
-                    count_strip<false>(S, a, T, C, slot, t, 2 * b + t, warp, lane, fx, lastmask, thr4, guard);
+                    count_strip<false, kIndep>(S, a, T, C, slot, t, 2 * b + t, warp, lane, fx, lastmask, thr4, guard);
                 else
-                    count_strip<true>(S, a, T, C, slot, t, 2 * b + t, warp, lane, fx, lastmask, thr4, guard);
+                    count_strip<true, kIndep>(S, a, T, C, slot, t, 2 * b + t, warp, lane, fx, lastmask, thr4, guard);
             }
         }
         __syncthreads();  // the next tile reuses ring slots and histories still read above
@@ -433,31 +498,42 @@ __global__ void __launch_bounds__(kTpb, 1) band_scan_kernel(const BandArgs a) {
     if (guard & 0x80808080u) atomicOr(a.overflow, 1u);
 }
 
-// Row-term table, one record of kRowWords words per (band group g, base row v), records of a
-// group contiguous: [m] = high part (>> 17) of the row term in band 32g + m (0 where the row lies
-// outside the area plus halo), [kRowLo] = its low 17 bits, [kRowValid] = number of bands of the
-// group that hold the row. Rows v >= vrows (padding) are all zero.
+// Row-term table, one record per (band group g, base row v), records of a group contiguous.
+// Band j = 32 g + m holds base row v at input row v + j * stride (stride 2^17 with the shared
+// LCG). Shared-LCG records (kRowWords): [m] = high part (>> 17) of the row term in band m (0 where
+// the row lies outside the area plus halo), [kRowLo] = its low 17 bits (the same in every band),
+// [kRowValid] = number of bands of the group that hold the row. Independent records
+// (kRowWordsI): [m] high part, [kRowLoI + m] low 17 bits, [kRowValidI] bands holding the row.
+// Rows v >= vrows (padding) are all zero.
+template <bool kIndep>
 __global__ void row_terms_kernel(uint32_t* rt, int32_t vrows_alloc, int32_t vrows, int32_t nj,
-                                 int32_t first, int64_t limit, int64_t seed, int32_t use_x_term) {
+                                 int32_t first, int64_t limit, int64_t stride, int64_t seed,
+                                 int32_t use_x_term) {
+    constexpr int kRW = row_words<kIndep>();
+    constexpr int kLo = kIndep ? kRowLoI : kRowLo;
+    constexpr int kValid = kIndep ? kRowValidI : kRowValid;
     const int32_t groups = (nj + kMaxBands - 1) / kMaxBands;
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (e >= (int64_t)groups * vrows_alloc * kRowWords) return;
-    const int32_t w = (int32_t)(e % kRowWords);
-    const int64_t rec = e / kRowWords;
+    if (e >= (int64_t)groups * vrows_alloc * kRW) return;
+    const int32_t w = (int32_t)(e % kRW);
+    const int64_t rec = e / kRW;
     const int32_t v = (int32_t)(rec % vrows_alloc), g = (int32_t)(rec / vrows_alloc);
     uint32_t out = 0;
     if (v < vrows) {
-        if (w < kMaxBands || w == kRowLo) {
-            const int32_t j = w == kRowLo ? 0 : g * kMaxBands + w;
-            const int64_t off = (int64_t)v + (int64_t)j * kPeriod;
+        const bool hi = w < kMaxBands;
+        const bool lo = kIndep ? (w >= kLo && w < kLo + kMaxBands) : w == kLo;
+        if (hi || lo) {
+            const int32_t m = hi ? w : kIndep ? w - kLo : 0;
+            const int32_t j = (!kIndep && lo) ? 0 : g * kMaxBands + m;
+            const int64_t off = (int64_t)v + (int64_t)j * stride;
             if (j < nj && off < limit) {
                 const int32_t c = (int32_t)((int64_t)first + off);
                 const uint64_t t = (use_x_term ? x_term(c) : z_term(c)) + (uint64_t)seed;
-                out = w == kRowLo ? (uint32_t)t & 0x1FFFFu : (uint32_t)(t >> kPeriodBits);
+                out = lo ? (uint32_t)t & 0x1FFFFu : (uint32_t)(t >> kPeriodBits);
             }
-        } else if (w == kRowValid) {
-            // bands j = 32g + m with v + j * 2^17 < limit, capped at the group's size
-            const int64_t jmax = (limit - 1 - v) / kPeriod;  // last band holding the row
+        } else if (w == kValid) {
+            // bands j = 32g + m with v + j * stride < limit, capped at the group's size
+            const int64_t jmax = (limit - 1 - v) / stride;  // last band holding the row
             const int64_t n = min((int64_t)nj, jmax + 1) - (int64_t)g * kMaxBands;
             out = (uint32_t)max((int64_t)0, min((int64_t)kMaxBands, n));
         }
@@ -479,32 +555,44 @@ int band_tile_out_w() { return kOutW; }
 int band_max_bands() { return kMaxBands; }
 
 cudaError_t band_prepare() {
-    cudaError_t e = cudaFuncSetAttribute(band_scan_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                         (int)sizeof(BandSmem));
-    if (e != cudaSuccess) return e;
-    return cudaFuncSetAttribute(band_scan_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)sizeof(BandSmem));
+    const int bytes = (int)sizeof(BandSmem);
+    cudaError_t e;
+    if ((e = cudaFuncSetAttribute(band_scan_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess ||
+        (e = cudaFuncSetAttribute(band_scan_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess ||
+        (e = cudaFuncSetAttribute(band_scan_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess)
+        return e;
+    return cudaFuncSetAttribute(band_scan_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
 cudaError_t launch_band_scan(const BandArgs& a, int grid, cudaStream_t s) {
-    if (a.mad_add)
-        band_scan_kernel<true><<<grid, kTpb, sizeof(BandSmem), s>>>(a);
-    else
-        band_scan_kernel<false><<<grid, kTpb, sizeof(BandSmem), s>>>(a);
+    const size_t bytes = sizeof(BandSmem);
+    if (a.indep) {
+        if (a.mad_add) band_scan_kernel<true, true><<<grid, kTpb, bytes, s>>>(a);
+        else band_scan_kernel<false, true><<<grid, kTpb, bytes, s>>>(a);
+    } else {
+        if (a.mad_add) band_scan_kernel<true, false><<<grid, kTpb, bytes, s>>>(a);
+        else band_scan_kernel<false, false><<<grid, kTpb, bytes, s>>>(a);
+    }
     return cudaGetLastError();
 }
 
-int band_row_words() { return kRowWords; }
+int band_row_words(bool indep) { return indep ? kRowWordsI : kRowWords; }
 
 cudaError_t launch_band_terms(uint64_t* ct, int32_t col_first, int32_t ncols, uint32_t* rt,
                               int32_t vrows_alloc, int32_t vrows, int32_t nj, int32_t row_first,
-                              int64_t row_limit, int64_t seed, bool transposed, cudaStream_t s) {
+                              int64_t row_limit, int64_t row_stride, int64_t seed, bool transposed,
+                              bool indep, cudaStream_t s) {
     // Columns carry no seed; rows carry it. Transposed searches swap which axis is x.
     col_terms_kernel<<<(ncols + 255) / 256, 256, 0, s>>>(ct, col_first, ncols, transposed ? 0 : 1);
     const int64_t groups = (nj + kMaxBands - 1) / kMaxBands;
-    const int64_t n = groups * vrows_alloc * kRowWords;
-    row_terms_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(rt, vrows_alloc, vrows, nj, row_first,
-                                                                row_limit, seed, transposed ? 1 : 0);
+    const int64_t n = groups * vrows_alloc * band_row_words(indep);
+    const unsigned blocks = (unsigned)((n + 255) / 256);
+    if (indep)
+        row_terms_kernel<true><<<blocks, 256, 0, s>>>(rt, vrows_alloc, vrows, nj, row_first, row_limit,
+                                                       row_stride, seed, transposed ? 1 : 0);
+    else
+        row_terms_kernel<false><<<blocks, 256, 0, s>>>(rt, vrows_alloc, vrows, nj, row_first, row_limit,
+                                                        row_stride, seed, transposed ? 1 : 0);
     return cudaGetLastError();
 }
 

@@ -66,26 +66,32 @@ def run(core, mode, *args, **kw):
         core.lib.slime_b200_set_engine(0, 0)
 
 
+# Engine modes: 2 = shared-LCG band engine, 3 = independent-band engine.
+ALGO = {2: 200, 3: 300}
+
+
+@pytest.mark.parametrize("mode", [2, 3])
 @pytest.mark.parametrize("idx", [0, 1, 2, 7])
-def test_band_engine_search_golden(core, golden, idx):
+def test_band_engine_search_golden(core, golden, idx, mode):
     g = golden["search"]
     name = str(g["names"][idx])
     seed, rd_max, lo, hi, rd_min, cx, cz, maxr, total = (int(v) for v in g["params"][idx])
     assert lo >= 28
-    got_total, got = run(core, 2, seed, rd_max, lo, hi, rd_min, cx, cz, maxr)
-    assert core.lib.get_gpu_v1_algorithm() == 200
+    got_total, got = run(core, mode, seed, rd_max, lo, hi, rd_min, cx, cz, maxr)
+    assert core.lib.get_gpu_v1_algorithm() == ALGO[mode]
     assert got_total == total, name
     assert np.array_equal(got, g[f"{name}_results"]), name
 
 
+@pytest.mark.parametrize("mode", [2, 3])
 @pytest.mark.parametrize("k,thr", [(0, 30), (1, 28), (2, 33), (3, 29)])
-def test_band_engine_planted_rare_chunk(core, oracle, k, thr):
+def test_band_engine_planted_rare_chunk(core, oracle, k, thr, mode):
     x, z = 123_457 + 17 * k, -98_765 - 11 * k
     seed = rare_seed(x, z, k)
     assert python_is_slime(seed, x, z)
     args = (seed, 60, thr, 221, 0, x + 5, z - 3, 5000)
     t_o, r_o = oracle.search(*args)
-    t_b, r_b = run(core, 2, *args)
+    t_b, r_b = run(core, mode, *args)
     assert core.lib.slime_b200_last_rare_chunks() >= 1
     assert t_b == t_o
     assert np.array_equal(r_b, r_o)
@@ -94,35 +100,40 @@ def test_band_engine_planted_rare_chunk(core, oracle, k, thr):
     assert t_g == t_o and np.array_equal(r_g, r_o)
 
 
-def test_band_engine_planted_rare_upper_bound(core, oracle):
+@pytest.mark.parametrize("mode", [2, 3])
+def test_band_engine_planted_rare_upper_bound(core, oracle, mode):
     x, z = -1_500_000, 1_400_000
     seed = rare_seed(x, z, 5)
     args = (seed, 40, 30, 34, 7, x, z, 2000)
     t_o, r_o = oracle.search(*args)
-    t_b, r_b = run(core, 2, *args)
+    t_b, r_b = run(core, mode, *args)
     assert t_b == t_o and np.array_equal(r_b, r_o)
 
 
+@pytest.mark.parametrize("mode", [2, 3])
 @pytest.mark.parametrize("case", [
     (20240607, 140_000, 54, 221, 0, 0, 0, 2000),          # 2 phases x 3 bands, wide tiles
     (-31337, 300_000, 57, 221, 0, 400_000, -250_000, 500),  # 5 x 5 periods, offset centre
     (77, 270_000, 50, 60, 90_000, -1_000_000, 1_000_000, 3000),  # upper bound + annulus
+    (5, 20_000, 45, 221, 0, 1_874_000, -1_874_000, 800),  # independent bands: 40,001^2 at the border
+    (9, 3_000, 38, 221, 0, -7, 7, 100_000),               # small area, many sites
 ])
-def test_band_vs_general_medium(core, case):
+def test_band_vs_general_medium(core, case, mode):
     t_g, r_g = run(core, 1, *case)
-    t_b, r_b = run(core, 2, *case)
+    t_b, r_b = run(core, mode, *case)
     assert t_b == t_g
     assert np.array_equal(r_b, r_g)
 
 
-def test_band_vs_general_low_threshold_millions_of_sites(core):
+@pytest.mark.parametrize("mode", [2, 3])
+def test_band_vs_general_low_threshold_millions_of_sites(core, mode):
     """Threshold 42 on a 280,001^2 area: 3.1 million sites, a survivor queue that overflows in
     every tile, and ~30 rare chunks whose distance test to far-away sites must not wrap."""
     from slime_b200 import workloads
     seed = workloads.full_world_scan().seed
     case = (seed, 140_000, 42, 221, 0, 0, 0, 4_000_000)
     t_g, r_g = run(core, 1, *case)
-    t_b, r_b = run(core, 2, *case)
+    t_b, r_b = run(core, mode, *case)
     assert t_g > 3_000_000
     assert core.lib.slime_b200_last_rare_chunks() > 0
     assert t_b == t_g
