@@ -162,6 +162,31 @@ int64_t slime_b200_search_noalloc(int64_t seed, int64_t rd_max, int32_t min_size
                                   int64_t rd_min, int32_t search_center_x, int32_t search_center_z,
                                   ExtChunkResult* results_buffer, int32_t max_results);
 
+/* ---- batched search (no reference counterpart) --------------------------------------------- */
+
+/* One search of a batch: the arguments of search_slime_clusters_gpu_v1_centered. 48 bytes. */
+typedef struct SlimeBatchRequest {
+    int64_t seed;
+    int64_t rd_max;
+    int64_t rd_min;
+    int32_t min_size;
+    int32_t max_size;
+    int32_t center_x;
+    int32_t center_z;
+    int32_t max_results;
+    int32_t precise_afk;
+} SlimeBatchRequest;
+
+/* Runs n searches as one batch. Searches with min_size >= 28 share one persistent launch of the
+ * independent-band kernel whose CTAs take the tiles of all of them from one device queue; the
+ * others (and any whose sites would not fit the batch's pool) run one by one. Request i writes
+ * min(total_i, max_results_i) ranked results at results + (max_results_0 + ... +
+ * max_results_{i-1}) and its total to totals[i], exactly as the single search would; totals[i]
+ * is -1 when request i's arguments are invalid. Returns 0, or -1 on a CUDA failure or a null
+ * buffer. No reference counterpart: the reference library runs one search per call. */
+int32_t slime_b200_search_batch(const SlimeBatchRequest* requests, int32_t n, ExtChunkResult* results,
+                                int64_t* totals);
+
 #ifdef __cplusplus
 }
 #endif

@@ -74,6 +74,14 @@ void Context::release() {
     outer.free();
     inner.free();
     y_ready = false;
+    bt_ct.free();
+    bt_rt.free();
+    bt_hits.free();
+    bt_rare.free();
+    bt_flags.free();
+    bt_counts.free();
+    bt_args.free();
+    bt_prefix.free();
     release_extra();
     if (pinned) cudaFreeHost(pinned);
     pinned = nullptr;
@@ -354,10 +362,20 @@ int64_t Context::search(const SearchSpec& q, ExtChunkResult* results) {
         progress.store(0);
         return -1;
     }
+    const int64_t total = finish(q, best, h, results);
+    if (total < 0) progress.store(0);
+    else progress.store(90);
+    return total;
+}
+
+int64_t Context::finish(const SearchSpec& q, std::vector<Hit>& best, const std::vector<uint32_t>& h,
+                        ExtChunkResult* results) {
     int64_t total = 0;
     for (int s = q.min_size; s <= q.max_size; ++s) total += h[s];
-    std::sort(best.begin(), best.end(), hit_better);
+    if (best.size() > (size_t)q.max_results)
+        std::nth_element(best.begin(), best.begin() + q.max_results, best.end(), hit_better);
     const int32_t n = (int32_t)std::min<size_t>(best.size(), (size_t)q.max_results);
+    std::sort(best.begin(), best.begin() + n, hit_better);
     for (int32_t i = 0; i < n; ++i) {
         ExtChunkResult& r = results[i];
         r.size = best[i].count;
@@ -369,12 +387,8 @@ int64_t Context::search(const SearchSpec& q, ExtChunkResult* results) {
     }
     if (q.precise_afk && !cancel.load() && n > 0) {
         // The search-time refinement covers the best 100 (SlimeCoreGPU.cu:3884).
-        if (!score(q.seed, results, std::min(n, 100), 1, y_enabled != 0)) {
-            progress.store(0);
-            return -1;
-        }
+        if (!score(q.seed, results, std::min(n, 100), 1, y_enabled != 0)) return -1;
     }
-    progress.store(90);
     return total;
 }
 
@@ -540,6 +554,19 @@ void slime_b200_set_engine(int32_t mode, int32_t band_min_threshold) {
 }
 
 const char* slime_b200_last_error(void) { return ctx().last_error.c_str(); }
+
+int32_t slime_b200_search_batch(const SlimeBatchRequest* requests, int32_t n, ExtChunkResult* results,
+                                int64_t* totals) {
+    std::lock_guard<std::mutex> lock(ctx().mu);
+    if (n < 0 || (n > 0 && (!requests || !results || !totals))) return -1;
+    std::vector<slime::SearchSpec> q((size_t)n);
+    for (int32_t i = 0; i < n; ++i) {
+        const SlimeBatchRequest& r = requests[i];
+        q[i] = slime::SearchSpec{r.seed, r.rd_max, r.min_size, r.max_size, r.rd_min, r.center_x, r.center_z,
+                                 r.max_results, r.precise_afk};
+    }
+    return ctx().search_batch(q.data(), n, reinterpret_cast<slime::ExtChunkResult*>(results), totals);
+}
 
 int32_t slime_b200_is_slime_batch(int64_t seed, const int64_t* x, const int64_t* z, uint8_t* out, int64_t n) {
     if (n <= 0) return 0;

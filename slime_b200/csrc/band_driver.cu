@@ -42,15 +42,48 @@ int32_t Context::engine_for(const SearchSpec& q) const {
     if (engine_override == 1 || q.min_size < 28) return kAlgoGeneral;
     if (engine_override == 2) return kAlgoBand;
     if (engine_override == 3) return kAlgoIndep;
-    // Measured on B200 (T centres/s, shared band / independent bands): radius 300k thr 50
-    // 0.76 / 1.00, thr 60 1.84 / -; radius 600k thr 50 1.06 / 1.02, thr 60 3.27 / 1.52. The shared
-    // LCG pays off with many periods or a high threshold.
+    // Measured on B200 (T centres/s, shared band / independent bands): radius 140k thr 50 0.49 /
+    // 1.02, thr 60 1.09 / 1.44; radius 300k thr 50 0.76 / 1.00, thr 60 1.84 / -; radius 600k thr
+    // 48 0.71 / 0.85, thr 50 1.17 / 1.09, thr 52 1.75 / 1.28, thr 55 2.56 / 1.43, thr 60 3.27 /
+    // 1.52. The shared LCG pays off with many periods (its work is shared by every band and
+    // phase pair) and a high threshold.
     const int64_t w = 2 * q.rd_max + 1;
-    if (w >= 2 * kP && q.min_size >= band_min_threshold &&
-        (q.min_size >= 55 || w >= 8 * kP))
+    if (q.min_size >= band_min_threshold && (w >= 7 * kP || (w >= 4 * kP && q.min_size >= 56)))
         return kAlgoBand;
     if (w * w >= indep_min_centres && q.min_size >= indep_min_threshold) return kAlgoIndep;
     return kAlgoGeneral;
+}
+
+BandGeom band_geometry(int64_t W, int64_t H, bool indep, int sm_count) {
+    BandGeom g{};
+    g.indep = indep;
+    g.transposed = !indep && W < 2 * kP && H >= 2 * kP;
+    g.width_u = g.transposed ? H : W;
+    g.height_v = g.transposed ? W : H;
+    const int out_w = band_tile_out_w();
+    const int nb_max = band_max_bands();
+    // Shared LCG: X phases and Z bands 2^17 apart. Independent bands: one phase, nJ bands of
+    // `stride` rows each (at least 256 rows a band, at most 32 bands).
+    g.nI = indep ? 1 : (g.width_u + kP - 1) / kP;
+    g.nJ = indep ? std::max<int64_t>(1, std::min<int64_t>(nb_max, g.height_v / 256)) : (g.height_v + kP - 1) / kP;
+    g.stride = indep ? (g.height_v + g.nJ - 1) / g.nJ : kP;
+    g.ubase = (int32_t)(indep ? g.width_u : std::min(kP, g.width_u));
+    g.vbase = (int32_t)std::min(g.stride, g.height_v);
+    g.vrows = g.vbase + 16;
+    g.vrows_alloc = g.vbase + 32;  // zero rows: 8-row bulk copies never run past the end
+    g.ngroups = (g.nJ + nb_max - 1) / nb_max;
+    g.u_tiles = (g.ubase + out_w - 1) / out_w;
+    g.band_h = (int32_t)std::min<int64_t>(2048, std::max<int64_t>(256, g.vbase));
+    if (indep) {
+        // Enough tiles for two waves of CTAs where the area allows it, tiles of 64+ rows.
+        const int64_t want = (2 * (int64_t)sm_count + g.u_tiles - 1) / g.u_tiles;
+        const int64_t vt = std::max<int64_t>((g.vbase + 2047) / 2048, std::min<int64_t>((g.vbase + 63) / 64, want));
+        g.band_h = (int32_t)((g.vbase + vt - 1) / vt);
+    }
+    g.v_tiles = (g.vbase + g.band_h - 1) / g.band_h;
+    g.pairs = (g.nI + 1) / 2;
+    g.tiles = g.u_tiles * g.v_tiles * g.pairs;
+    return g;
 }
 
 bool Context::scan_band(const SearchSpec& q, std::vector<Hit>& best, std::vector<uint32_t>& h,
@@ -59,21 +92,13 @@ bool Context::scan_band(const SearchSpec& q, std::vector<Hit>& best, std::vector
     const int64_t W = 2 * q.rd_max + 1, H = W;
     const int32_t area_x0 = (int32_t)((int64_t)q.center_x - q.rd_max);
     const int32_t area_z0 = (int32_t)((int64_t)q.center_z - q.rd_max);
-    const bool transposed = !indep && W < 2 * kP && H >= 2 * kP;
-    const int64_t width_u = transposed ? H : W, height_v = transposed ? W : H;
-    const int out_w = band_tile_out_w();
+    const BandGeom G = band_geometry(W, H, indep, sm_count);
+    const bool transposed = G.transposed;
+    const int64_t width_u = G.width_u, height_v = G.height_v;
     const int nb_max = band_max_bands();
-    // Shared LCG: X phases and Z bands 2^17 apart. Independent bands: one phase, nJ bands of
-    // `stride` rows each (at least 256 rows a band, at most 32 bands).
-    const int64_t nI = indep ? 1 : (width_u + kP - 1) / kP;
-    const int64_t nJ = indep ? std::max<int64_t>(1, std::min<int64_t>(nb_max, height_v / 256))
-                             : (height_v + kP - 1) / kP;
-    const int64_t stride = indep ? (height_v + nJ - 1) / nJ : kP;
-    const int32_t ubase = (int32_t)(indep ? width_u : std::min(kP, width_u));
-    const int32_t vbase = (int32_t)std::min(stride, height_v);
-    const int32_t vrows = vbase + 16;
-    const int32_t vrows_alloc = vbase + 32;  // zero rows: 8-row bulk copies never run past the end
-    const int64_t ngroups = (nJ + nb_max - 1) / nb_max;
+    const int64_t nJ = G.nJ, stride = G.stride;
+    const int32_t ubase = G.ubase, vbase = G.vbase, vrows = G.vrows, vrows_alloc = G.vrows_alloc;
+    const int64_t ngroups = G.ngroups;
     cudaError_t e;
     if ((e = xt.reserve((size_t)width_u + 16)) != cudaSuccess ||
         (e = rt.reserve((size_t)ngroups * vrows_alloc * band_row_words(indep))) != cudaSuccess ||
@@ -108,17 +133,8 @@ bool Context::scan_band(const SearchSpec& q, std::vector<Hit>& best, std::vector
     if (nrare > kRareCap) { set_error("too many rare chunks", cudaErrorMemoryAllocation); return false; }
     last_rare = nrare;
 
-    const int64_t u_tiles = (ubase + out_w - 1) / out_w;
-    int32_t band_h = (int32_t)std::min<int64_t>(2048, std::max<int64_t>(256, vbase));
-    if (indep) {
-        // Enough tiles for two waves of CTAs where the area allows it, tiles of 64+ rows.
-        const int64_t want = (2 * (int64_t)sm_count + u_tiles - 1) / u_tiles;
-        const int64_t vt = std::max<int64_t>((vbase + 2047) / 2048,
-                                             std::min<int64_t>((vbase + 63) / 64, want));
-        band_h = (int32_t)((vbase + vt - 1) / vt);
-    }
-    const int64_t v_tiles = (vbase + band_h - 1) / band_h;
-    const int64_t pairs = (nI + 1) / 2;
+    const int64_t u_tiles = G.u_tiles, v_tiles = G.v_tiles;
+    const int32_t band_h = G.band_h;
     const int grid = sm_count;
     const uint64_t cap = hits.count;
 
@@ -126,7 +142,7 @@ bool Context::scan_band(const SearchSpec& q, std::vector<Hit>& best, std::vector
         const int32_t j0 = (int32_t)(g * nb_max);
         const int32_t nb = (int32_t)std::min<int64_t>(nb_max, nJ - j0);
         if (nb <= 0) break;
-        const int64_t tiles = u_tiles * v_tiles * pairs;
+        const int64_t tiles = G.tiles;
         int64_t chunk = std::max<int64_t>(grid, std::min<int64_t>(tiles, (int64_t)grid * 24));
         for (int64_t t0 = 0; t0 < tiles;) {
             while (paused.load() && !cancel.load()) std::this_thread::sleep_for(std::chrono::milliseconds(20));

@@ -9,6 +9,7 @@
 
 #include <cuda_runtime.h>
 
+#include "engine.h"
 #include "slime_core.cuh"
 
 namespace slime {
@@ -96,12 +97,22 @@ struct Context {
     DeviceBuffer<int2> rare;
     DeviceBuffer<Hit> fixed;
     DeviceBuffer<unsigned int> flags;  // [0] overflow, [1] fix-up error, [2] rare count
+
+    // Batched searches (batch.cu): pools of all searches of a batch, sliced per search.
+    DeviceBuffer<uint64_t> bt_ct;
+    DeviceBuffer<uint32_t> bt_rt;
+    DeviceBuffer<Hit> bt_hits;
+    DeviceBuffer<int2> bt_rare;
+    DeviceBuffer<unsigned int> bt_flags;          // per search: overflow, fix-up error, rare count, spare
+    DeviceBuffer<unsigned long long> bt_counts;   // per search: emitted, fixed; then the tile queue
+    DeviceBuffer<BandArgs> bt_args;
+    DeviceBuffer<int64_t> bt_prefix;
     bool band_ready = false;
     int32_t engine_override = 0;       // 0 auto, 1 general scan, 2 band engine, 3 independent bands
     // Auto mode uses the shared-LCG band engine from this threshold: below it the exact counts of
-    // the many surviving 4x4 groups dominate (B200 crossover with the general scan measured
-    // between 45 and 48 on a 1,200,001^2 area).
-    int32_t band_min_threshold = 48;
+    // the many surviving 4x4 groups dominate and independent bands are faster (B200 crossover
+    // between 48 and 50 on a 1,200,001^2 area).
+    int32_t band_min_threshold = 50;
     // Auto mode uses the independent-band engine for areas of at least this many centres from
     // this threshold on.
     int32_t indep_min_threshold = 44;
@@ -143,6 +154,11 @@ struct Context {
                    bool& cancelled, bool indep);
     bool score(int64_t seed, ExtChunkResult* host, int32_t n, int32_t scan_xz, bool pack);
     int64_t search(const SearchSpec& q, ExtChunkResult* results);
+    // Total in range, ranked results and precise scores of a finished scan (-1 on failure).
+    int64_t finish(const SearchSpec& q, std::vector<Hit>& best, const std::vector<uint32_t>& h,
+                   ExtChunkResult* results);
+    // Many searches: those the independent-band kernel can take share one persistent launch.
+    int32_t search_batch(const SearchSpec* q, int32_t n, ExtChunkResult* results, int64_t* totals);
 };
 
 Context& ctx();

@@ -91,11 +91,26 @@ struct BandArgs {
     int64_t row_stride;      // input rows between band j and band j + 1 (2^17 with the shared LCG)
 };
 
+// Tiling of one band search (band_driver.cu): axes (u = phase axis, v = band axis), phases,
+// bands, base sizes and tiles, as the band kernels expect them.
+struct BandGeom {
+    bool indep, transposed;
+    int64_t width_u, height_v, nI, nJ, stride, ngroups;
+    int32_t ubase, vbase, vrows, vrows_alloc, band_h;
+    int64_t u_tiles, v_tiles, pairs, tiles;
+};
+BandGeom band_geometry(int64_t W, int64_t H, bool indep, int sm_count);
+
 size_t band_smem_bytes();
 int band_tile_out_w();
 int band_max_bands();
 cudaError_t band_prepare();
 cudaError_t launch_band_scan(const BandArgs& a, int grid, cudaStream_t s);
+// Tiles of many band searches in one launch: args[i] (device) describes search i (either mode),
+// prefix[i] (device, nsearch + 1 entries) is its first tile in the batch, *head (device, zeroed)
+// is the tile queue. Each search's tile_begin/tile_end are unused.
+cudaError_t launch_band_batch(const BandArgs* args, const int64_t* prefix, int32_t nsearch,
+                              unsigned long long* head, bool mad_add, int grid, cudaStream_t s);
 int band_row_words(bool indep);
 cudaError_t launch_band_terms(uint64_t* ct, int32_t col_first, int32_t ncols, uint32_t* rt,
                               int32_t vrows_alloc, int32_t vrows, int32_t nj, int32_t row_first,

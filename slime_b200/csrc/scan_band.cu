@@ -62,6 +62,9 @@ struct __align__(16) BandSmem {
     uint32_t hist_o[5][kMaxCombos][kWords];   // (odd groups)
     uint32_t rows[3][kBatchRows * kRowWordsI];  // row terms of 3 batches, filled by bulk copies
     unsigned long long rows_bar[3];           // mbarriers of the three row-term buffers
+    BandArgs args;                            // batched kernel: the current tile's search
+    long long next_tile;                      // batched kernel: tile taken from the queue
+    int search;                               // batched kernel: its search
     int failed;  // a bounded wait gave up: the CTA stops
 };
 
@@ -151,13 +154,17 @@ __device__ __forceinline__ void exact_group(const BandSmem& S, const BandArgs& a
         }
         slice = __funnelshift_r(lo, hi, 4 * g) & 0xFFFFFu;
     }
-    const int dx = lane & 3, dz = (lane >> 2) & 3;
+    // Lane l counts window rows 0..8 (l < 16) or 9..16 (l >= 16) of centre l % 16; the halves
+    // are then added across the two half-warps.
+    const int dx = lane & 3, dz = (lane >> 2) & 3, half = lane >> 4;
     int count = 0;
 #pragma unroll
-    for (int i = 0; i < 17; ++i) {
-        const uint32_t row = __shfl_sync(kFull, slice, dz + i);
-        count += __popc((row >> dx) & window_row_mask(i));
+    for (int k = 0; k < 9; ++k) {
+        const uint32_t row = __shfl_sync(kFull, slice, dz + 9 * half + k);
+        const uint32_t mask = half ? (k < 8 ? window_row_mask(9 + k) : 0u) : window_row_mask(k);
+        count += __popc((row >> dx) & mask);
     }
+    count += __shfl_xor_sync(kFull, count, 16);
     bool keep = false;
     int cx = 0, cz = 0;
     if (lane < 16) {
@@ -299,32 +306,33 @@ __device__ __forceinline__ bool indep_hit(uint32_t xl, uint32_t xh, uint32_t zl,
     return !(t & 1u) && t * kTwoInv5 < kHitBelow;
 }
 
-template <bool kMadAdd, bool kIndep>
-__global__ void __launch_bounds__(kTpb, 1) band_scan_kernel(const BandArgs a) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    BandSmem& S = *reinterpret_cast<BandSmem*>(smem_raw);
-    const int tid = threadIdx.x, lane = tid & 31;
-    const int warp = __shfl_sync(kFull, tid >> 5, 0);  // warp-uniform for the compiler
-    const int nb = a.nb;
-    const uint32_t thr4 = (uint32_t)min(a.min_size, 128) * 0x01010101u;
-    const uint32_t one = a.one;  // 1 at run time: keeps the band add on the multiply pipe
-    uint32_t guard = 0;
-    uint32_t bar_phase = 0;  // bit r: parity of the next completion of rows_bar[r]
+// CTA set-up shared by the kernels: mbarriers and a zeroed ring (with the shared LCG, planes of
+// bands beyond nb are never generated: they stay zero and count nothing).
+__device__ __forceinline__ void band_cta_init(BandSmem& S, int tid) {
     if (tid == 0) {
         S.failed = 0;
         for (int r = 0; r < 3; ++r)
             asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" :: "r"(smem_u32(&S.rows_bar[r])) : "memory");
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    // Planes of bands beyond nb are never generated: they stay zero and count nothing.
     for (int i = tid; i < kRingSlots * kBatchRows * kPlanes * kWords; i += kTpb) (&S.ring[0][0][0][0])[i] = 0;
+    __syncthreads();
+}
+
+// One tile of one search (block-uniform arguments; all threads). Returns false when a bounded
+// wait gave up (the search's overflow word gets bit 4 and the CTA must stop).
+template <bool kMadAdd, bool kIndep>
+__device__ __forceinline__ bool band_tile(BandSmem& S, const BandArgs& a, int64_t tile, int tid, int lane,
+                                          int warp, uint32_t& bar_phase) {
+    const int nb = a.nb;
+    const uint32_t thr4 = (uint32_t)min(a.min_size, 128) * 0x01010101u;
+    const uint32_t one = a.one;  // 1 at run time: keeps the band add on the multiply pipe
     // Counter constants: the swap sense of the warp's phase and the groups lane 31 may flag
     // (groups 4..7 of word 31 hold centres 1,008+ of the tile, which belong to the next tile).
     const uint32_t fx = ((warp ^ (warp >> 1)) & 1) ? 0u : ~0u;
     const uint32_t lastmask = lane == kWords - 1 ? 0x0000C0C0u : ~0u;
-    __syncthreads();
-
-    for (int64_t tile = a.tile_begin + blockIdx.x; tile < a.tile_end; tile += gridDim.x) {
+    uint32_t guard = 0;
+    {
         Tile T;
         const int ut = (int)(tile % a.u_tiles);
         const int64_t rest = tile / a.u_tiles;
@@ -335,7 +343,7 @@ __global__ void __launch_bounds__(kTpb, 1) band_scan_kernel(const BandArgs a) {
         // Tiles with no centre of the area in any of their combos are skipped (block-uniform).
         if ((int64_t)T.u0 + (int64_t)T.i0 * kPeriod >= a.width_u ||
             (int64_t)T.v0 + (int64_t)a.j0 * a.row_stride >= a.height_v)
-            continue;
+            return true;
         T.out_h = min(a.band_h, a.vbase - T.v0);
         const int strips = (T.out_h + 16 + 3) / 4;
         const int batches = (strips + 1) / 2;
@@ -476,7 +484,7 @@ __global__ void __launch_bounds__(kTpb, 1) band_scan_kernel(const BandArgs a) {
             }
             }
             __syncthreads();
-            if (S.failed) return;  // block-uniform after the barrier
+            if (S.failed) return false;  // block-uniform after the barrier
 
             // Row terms of batch b + 2 (its buffer was last read before this batch's barrier).
             if (tid == kTpb - 32 && b + 2 < batches)
@@ -496,6 +504,76 @@ __global__ void __launch_bounds__(kTpb, 1) band_scan_kernel(const BandArgs a) {
     }
     // A 4-row strip with 52+ hits among its 80 cells could carry a box past a byte lane.
     if (guard & 0x80808080u) atomicOr(a.overflow, 1u);
+    return true;
+}
+
+template <bool kMadAdd, bool kIndep>
+__global__ void __launch_bounds__(kTpb, 1) band_scan_kernel(const BandArgs a) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    BandSmem& S = *reinterpret_cast<BandSmem*>(smem_raw);
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int warp = __shfl_sync(kFull, tid >> 5, 0);  // warp-uniform for the compiler
+    uint32_t bar_phase = 0;  // bit r: parity of the next completion of rows_bar[r]
+    band_cta_init(S, tid);
+    for (int64_t tile = a.tile_begin + blockIdx.x; tile < a.tile_end; tile += gridDim.x)
+        if (!band_tile<kMadAdd, kIndep>(S, a, tile, tid, lane, warp, bar_phase)) return;
+}
+
+// Many searches in one persistent launch (each search independent-band or shared-LCG): each CTA
+// takes the next tile of the whole batch from a device counter, finds its search in the tile
+// prefix sums and copies that search's arguments into shared memory. Stale planes of a previous
+// search with more bands are never read by the independent-band counter (it skips combos beyond
+// the band count) and are cleared before a shared-LCG tile.
+template <bool kMadAdd>
+__global__ void __launch_bounds__(kTpb, 1) band_batch_kernel(const BandArgs* args, const int64_t* prefix,
+                                                             int32_t nsearch, unsigned long long* head) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    BandSmem& S = *reinterpret_cast<BandSmem*>(smem_raw);
+    const int tid = threadIdx.x, lane = tid & 31;
+    const int warp = __shfl_sync(kFull, tid >> 5, 0);
+    uint32_t bar_phase = 0;
+    band_cta_init(S, tid);
+    const int64_t total = prefix[nsearch];
+    for (;;) {
+        if (tid == 0) {
+            const long long t = (long long)atomicAdd(head, 1ull);
+            int lo = 0, hi = nsearch - 1;  // last search whose first tile is <= t
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (prefix[mid] <= t) lo = mid; else hi = mid - 1;
+            }
+            S.next_tile = t;
+            S.search = lo;
+        }
+        __syncthreads();
+        const int64_t t = S.next_tile;
+        if (t >= total) return;  // block-uniform
+        const int s = S.search;
+        constexpr int kArgWords = (int)(sizeof(BandArgs) / 4);
+        for (int i = tid; i < kArgWords; i += kTpb)
+            reinterpret_cast<uint32_t*>(&S.args)[i] = reinterpret_cast<const uint32_t*>(&args[s])[i];
+        __syncthreads();
+        bool ok;
+        if (S.args.indep) {
+            ok = band_tile<kMadAdd, true>(S, S.args, t - prefix[s], tid, lane, warp, bar_phase);
+        } else {
+            // The shared-LCG counter reads every plane: clear planes of bands this search does
+            // not generate (a previous search may have left bits there).
+            for (int i = tid; i < kRingSlots * kBatchRows * kMaxBands * kWords; i += kTpb) {
+                const int m = (i / kWords) % kMaxBands;
+                if (m >= S.args.nb) {
+                    const int w = i % kWords, r = i / (kWords * kMaxBands);
+                    S.ring[r / kBatchRows][r % kBatchRows][m][w] = 0;
+                }
+            }
+            __syncthreads();
+            ok = band_tile<kMadAdd, false>(S, S.args, t - prefix[s], tid, lane, warp, bar_phase);
+        }
+        if (!ok) {
+            if (tid == 0) atomicOr(S.args.overflow, 4u);
+            return;
+        }
+    }
 }
 
 // Row-term table, one record per (band group g, base row v), records of a group contiguous.
@@ -559,9 +637,19 @@ cudaError_t band_prepare() {
     cudaError_t e;
     if ((e = cudaFuncSetAttribute(band_scan_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess ||
         (e = cudaFuncSetAttribute(band_scan_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess ||
-        (e = cudaFuncSetAttribute(band_scan_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess)
+        (e = cudaFuncSetAttribute(band_scan_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess ||
+        (e = cudaFuncSetAttribute(band_scan_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess ||
+        (e = cudaFuncSetAttribute(band_batch_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess)
         return e;
-    return cudaFuncSetAttribute(band_scan_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    return cudaFuncSetAttribute(band_batch_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+}
+
+cudaError_t launch_band_batch(const BandArgs* args, const int64_t* prefix, int32_t nsearch,
+                              unsigned long long* head, bool mad_add, int grid, cudaStream_t s) {
+    const size_t bytes = sizeof(BandSmem);
+    if (mad_add) band_batch_kernel<true><<<grid, kTpb, bytes, s>>>(args, prefix, nsearch, head);
+    else band_batch_kernel<false><<<grid, kTpb, bytes, s>>>(args, prefix, nsearch, head);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_band_scan(const BandArgs& a, int grid, cudaStream_t s) {

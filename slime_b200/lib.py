@@ -56,7 +56,15 @@ SIGNATURES = {
     "slime_b200_set_tuning": (None, [i32]),
     "slime_b200_microbench": (i32, [i32, i32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "slime_b200_search_noalloc": (i64, [i64, i64, i32, i32, i64, i32, i32, vp, i32]),
+    "slime_b200_search_batch": (i32, [vp, i32, vp, vp]),
 }
+
+# SlimeBatchRequest (48 bytes): the arguments of one search of a batch.
+REQUEST_DTYPE = np.dtype(
+    [("seed", "<i8"), ("rd_max", "<i8"), ("rd_min", "<i8"), ("min_size", "<i4"),
+     ("max_size", "<i4"), ("center_x", "<i4"), ("center_z", "<i4"), ("max_results", "<i4"),
+     ("precise_afk", "<i4")]
+)
 
 
 def load(path: Path | str = LIB) -> C.CDLL:
@@ -99,6 +107,25 @@ class SlimeCoreB200:
             precise_afk)
         self._check(total >= 0, "search")
         return total, buf[: min(total, max_results)]
+
+    def search_batch(self, searches):
+        """slime_b200_search_batch over objects with the fields of workloads.Search; returns a
+        list of (total, ranked results), one per search."""
+        req = np.zeros(len(searches), dtype=REQUEST_DTYPE)
+        for i, q in enumerate(searches):
+            req[i] = (q.seed, q.radius, q.rd_min, q.min_size, q.max_size, q.center_x, q.center_z,
+                      q.max_results, q.precise_afk)
+        offs = np.concatenate([[0], np.cumsum(req["max_results"].astype(np.int64))])
+        buf = np.zeros(max(int(offs[-1]), 1), dtype=RESULT_DTYPE)
+        totals = np.zeros(max(len(searches), 1), dtype=np.int64)
+        rc = self.lib.slime_b200_search_batch(_ptr(req), len(searches), _ptr(buf), _ptr(totals))
+        self._check(rc == 0, "search_batch")
+        out = []
+        for i in range(len(searches)):
+            t = int(totals[i])
+            n = 0 if t < 0 else min(t, int(req["max_results"][i]))
+            out.append((t, buf[offs[i]:offs[i] + n].copy()))
+        return out
 
     def score_precise(self, seed: int, sites: np.ndarray, scan_xz: int = 1) -> np.ndarray:
         buf = np.ascontiguousarray(sites, dtype=RESULT_DTYPE).copy()
