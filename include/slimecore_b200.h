@@ -187,6 +187,36 @@ typedef struct SlimeBatchRequest {
 int32_t slime_b200_search_batch(const SlimeBatchRequest* requests, int32_t n, ExtChunkResult* results,
                                 int64_t* totals);
 
+/* ---- search server (no reference counterpart) ----------------------------------------------- */
+
+/* A server runs submitted searches on a worker thread with continuous batching: each step admits
+ * queued requests in arrival order while the device memory they need fits `device_bytes`, then
+ * runs a quantum of tiles (about `tiles_per_step` in all; <= 0 picks 4 per SM) of every admitted
+ * band-engine search in one persistent launch, finishing those whose last tile ran. Requests for
+ * the general scan (thresholds below the band engines' range) run whole within a step. Results
+ * are exactly those of search_slime_clusters_gpu_v1_centered for the same arguments. Returns an
+ * opaque handle, or NULL without a usable device. */
+void* slime_b200_server_create(int64_t device_bytes, int32_t tiles_per_step);
+
+/* Queues one request; returns its ticket (>= 0), or -1 for invalid arguments. */
+int64_t slime_b200_server_submit(void* server, const SlimeBatchRequest* request);
+
+/* State of a ticket: 0 queued, 1 running, 2 done, -1 failed (e.g. it needs more device memory
+ * than the server's budget), -2 unknown ticket. */
+int32_t slime_b200_server_poll(void* server, int64_t ticket);
+
+/* Waits up to timeout_ms for a ticket to finish; returns its state as slime_b200_server_poll. */
+int32_t slime_b200_server_wait(void* server, int64_t ticket, int32_t timeout_ms);
+
+/* For a finished ticket: writes min(total, capacity, max_results) ranked results, the time from
+ * submission to completion in ms, forgets the ticket and returns the total (-1 if it failed).
+ * Returns -2 (ticket kept) while it is not finished, or for an unknown ticket. */
+int64_t slime_b200_server_take(void* server, int64_t ticket, ExtChunkResult* results, int32_t capacity,
+                               double* latency_ms);
+
+/* Stops the worker (unfinished tickets fail), releases the server's device memory and the handle. */
+void slime_b200_server_destroy(void* server);
+
 #ifdef __cplusplus
 }
 #endif

@@ -50,6 +50,60 @@ constexpr uint64_t kHitCapMax = 16ull << 20;    // per search; larger searches r
 
 }  // namespace
 
+bool Context::collect_band(const SearchSpec& q, int32_t area_x0, int32_t area_z0, const Hit* hits_host,
+                           uint64_t n, const int2* rare_dev, uint32_t nrare, unsigned long long* fixed_count_dev,
+                           unsigned int* ferr_dev, std::vector<Hit>& best, std::vector<uint32_t>& h) {
+    std::fill(h.begin(), h.end(), 0u);
+    best.clear();
+    best.reserve(n);
+    for (uint64_t k = 0; k < n; ++k) {
+        const Hit& hit = hits_host[k];
+        if (hit.count < 0) continue;  // window holds a rare chunk: fixed below
+        ++h[hit.count];
+        best.push_back(hit);
+    }
+    if (!nrare) return true;
+    FixArgs f{};
+    f.area_x0 = area_x0;
+    f.area_z0 = area_z0;
+    f.width = 2 * q.rd_max + 1;
+    f.height = 2 * q.rd_max + 1;
+    f.rd_min_sq = q.rd_min * q.rd_min;
+    f.center_x = q.center_x;
+    f.center_z = q.center_z;
+    f.min_size = q.min_size;
+    f.max_size = q.max_size;
+    f.fixed = fixed.ptr;
+    f.fixed_count = fixed_count_dev;
+    f.cap = fixed.count;
+    f.error = ferr_dev;
+    cudaError_t e;
+    uint64_t nf = 0;
+    uint32_t ferr = 0;
+    if ((e = cudaMemsetAsync(fixed_count_dev, 0, 8, stream)) != cudaSuccess ||
+        (e = cudaMemsetAsync(ferr_dev, 0, 4, stream)) != cudaSuccess ||
+        (e = launch_fixup(rare_dev, (int32_t)nrare, q.seed, f, stream)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(&nf, fixed_count_dev, 8, cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(&ferr, ferr_dev, 4, cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(stream)) != cudaSuccess) {
+        set_error("fixup", e);
+        return false;
+    }
+    ++last_launches;
+    if (nf > fixed.count || ferr) { set_error("fixup overflow", cudaErrorUnknown); return false; }
+    if (nf) {
+        const size_t old = best.size();
+        best.resize(old + nf);
+        if ((e = cudaMemcpyAsync(best.data() + old, fixed.ptr, nf * sizeof(Hit), cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
+            (e = cudaStreamSynchronize(stream)) != cudaSuccess) {
+            set_error("copy", e);
+            return false;
+        }
+        for (size_t k = old; k < best.size(); ++k) ++h[best[k].count];
+    }
+    return true;
+}
+
 int32_t Context::search_batch(const SearchSpec* reqs, int32_t n, ExtChunkResult* results, int64_t* totals) {
     if (n < 0 || (n > 0 && (!reqs || !results || !totals))) {
         last_error = "batch: invalid arguments";
@@ -243,54 +297,10 @@ int32_t Context::search_batch(const SearchSpec* reqs, int32_t n, ExtChunkResult*
             alone.push_back(p.idx);
             continue;
         }
-        std::fill(h.begin(), h.end(), 0u);
         std::vector<Hit> best;
-        best.reserve(emitted[s]);
-        for (uint64_t k = 0; k < emitted[s]; ++k) {
-            const Hit& hit = hits_h[p.hit_off + k];
-            if (hit.count < 0) continue;  // window holds a rare chunk: fixed below
-            ++h[hit.count];
-            best.push_back(hit);
-        }
-        const uint32_t nrare = flags_h[4 * s + 2];
-        if (nrare) {
-            FixArgs f{};
-            f.area_x0 = p.area_x0;
-            f.area_z0 = p.area_z0;
-            f.width = 2 * q.rd_max + 1;
-            f.height = 2 * q.rd_max + 1;
-            f.rd_min_sq = q.rd_min * q.rd_min;
-            f.center_x = q.center_x;
-            f.center_z = q.center_z;
-            f.min_size = q.min_size;
-            f.max_size = q.max_size;
-            f.fixed = fixed.ptr;
-            f.fixed_count = bt_counts.ptr + 2 * s + 1;
-            f.cap = fixed.count;
-            f.error = bt_flags.ptr + 4 * s + 1;
-            cudaError_t e;
-            uint64_t nf = 0;
-            uint32_t ferr = 0;
-            if ((e = launch_fixup(bt_rare.ptr + p.rare_off, (int32_t)nrare, q.seed, f, stream)) != cudaSuccess ||
-                (e = cudaMemcpyAsync(&nf, bt_counts.ptr + 2 * s + 1, 8, cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
-                (e = cudaMemcpyAsync(&ferr, bt_flags.ptr + 4 * s + 1, 4, cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
-                (e = cudaStreamSynchronize(stream)) != cudaSuccess) {
-                set_error("batch fixup", e);
-                return -1;
-            }
-            ++last_launches;
-            if (nf > fixed.count || ferr) { set_error("fixup overflow", cudaErrorUnknown); return -1; }
-            if (nf) {
-                const size_t old = best.size();
-                best.resize(old + nf);
-                if ((e = cudaMemcpyAsync(best.data() + old, fixed.ptr, nf * sizeof(Hit), cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
-                    (e = cudaStreamSynchronize(stream)) != cudaSuccess) {
-                    set_error("batch copy", e);
-                    return -1;
-                }
-                for (size_t k = old; k < best.size(); ++k) ++h[best[k].count];
-            }
-        }
+        if (!collect_band(q, p.area_x0, p.area_z0, hits_h.data() + p.hit_off, emitted[s], bt_rare.ptr + p.rare_off,
+                          flags_h[4 * s + 2], bt_counts.ptr + 2 * s + 1, bt_flags.ptr + 4 * s + 1, best, h))
+            return -1;
         const int64_t total = finish(q, best, h, results + res_off[p.idx]);
         if (total < 0) return -1;
         totals[p.idx] = total;

@@ -159,6 +159,11 @@ struct Context {
                    ExtChunkResult* results);
     // Many searches: those the independent-band kernel can take share one persistent launch.
     int32_t search_batch(const SearchSpec* q, int32_t n, ExtChunkResult* results, int64_t* totals);
+    // Sites and histogram of a finished band search from its emitted hits (already filtered
+    // against its rare chunks on the device) plus the rare-chunk fix-up.
+    bool collect_band(const SearchSpec& q, int32_t area_x0, int32_t area_z0, const Hit* hits_host, uint64_t n,
+                      const int2* rare_dev, uint32_t nrare, unsigned long long* fixed_count_dev,
+                      unsigned int* ferr_dev, std::vector<Hit>& best, std::vector<uint32_t>& h);
 };
 
 Context& ctx();

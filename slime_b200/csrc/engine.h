@@ -108,7 +108,8 @@ cudaError_t band_prepare();
 cudaError_t launch_band_scan(const BandArgs& a, int grid, cudaStream_t s);
 // Tiles of many band searches in one launch: args[i] (device) describes search i (either mode),
 // prefix[i] (device, nsearch + 1 entries) is its first tile in the batch, *head (device, zeroed)
-// is the tile queue. Each search's tile_begin/tile_end are unused.
+// is the tile queue. Item i runs tiles tile_begin .. tile_begin + prefix[i+1] - prefix[i] - 1 of
+// its search (tile_end is unused).
 cudaError_t launch_band_batch(const BandArgs* args, const int64_t* prefix, int32_t nsearch,
                               unsigned long long* head, bool mad_add, int grid, cudaStream_t s);
 int band_row_words(bool indep);

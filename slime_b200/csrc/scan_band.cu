@@ -521,7 +521,8 @@ __global__ void __launch_bounds__(kTpb, 1) band_scan_kernel(const BandArgs a) {
 
 // Many searches in one persistent launch (each search independent-band or shared-LCG): each CTA
 // takes the next tile of the whole batch from a device counter, finds its search in the tile
-// prefix sums and copies that search's arguments into shared memory. Stale planes of a previous
+// prefix sums and copies that search's arguments into shared memory. Work item i covers tiles
+// args[i].tile_begin .. + (prefix[i+1] - prefix[i]) of its search. Stale planes of a previous
 // search with more bands are never read by the independent-band counter (it skips combos beyond
 // the band count) and are cleared before a shared-LCG tile.
 template <bool kMadAdd>
@@ -555,7 +556,7 @@ __global__ void __launch_bounds__(kTpb, 1) band_batch_kernel(const BandArgs* arg
         __syncthreads();
         bool ok;
         if (S.args.indep) {
-            ok = band_tile<kMadAdd, true>(S, S.args, t - prefix[s], tid, lane, warp, bar_phase);
+            ok = band_tile<kMadAdd, true>(S, S.args, S.args.tile_begin + t - prefix[s], tid, lane, warp, bar_phase);
         } else {
             // The shared-LCG counter reads every plane: clear planes of bands this search does
             // not generate (a previous search may have left bits there).
@@ -567,7 +568,7 @@ __global__ void __launch_bounds__(kTpb, 1) band_batch_kernel(const BandArgs* arg
                 }
             }
             __syncthreads();
-            ok = band_tile<kMadAdd, false>(S, S.args, t - prefix[s], tid, lane, warp, bar_phase);
+            ok = band_tile<kMadAdd, false>(S, S.args, S.args.tile_begin + t - prefix[s], tid, lane, warp, bar_phase);
         }
         if (!ok) {
             if (tid == 0) atomicOr(S.args.overflow, 4u);

@@ -57,6 +57,12 @@ SIGNATURES = {
     "slime_b200_microbench": (i32, [i32, i32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "slime_b200_search_noalloc": (i64, [i64, i64, i32, i32, i64, i32, i32, vp, i32]),
     "slime_b200_search_batch": (i32, [vp, i32, vp, vp]),
+    "slime_b200_server_create": (vp, [i64, i32]),
+    "slime_b200_server_submit": (i64, [vp, vp]),
+    "slime_b200_server_poll": (i32, [vp, i64]),
+    "slime_b200_server_wait": (i32, [vp, i64, i32]),
+    "slime_b200_server_take": (i64, [vp, i64, vp, i32, C.POINTER(C.c_double)]),
+    "slime_b200_server_destroy": (None, [vp]),
 }
 
 # SlimeBatchRequest (48 bytes): the arguments of one search of a batch.
@@ -158,3 +164,59 @@ class SlimeCoreB200:
         self._check(self.lib.slime_b200_microbench(kind, iters, C.byref(ops), C.byref(ms)) == 0,
                     "microbench")
         return ops.value, ms.value
+
+
+def _request(q) -> np.ndarray:
+    req = np.zeros(1, dtype=REQUEST_DTYPE)
+    req[0] = (q.seed, q.radius, q.rd_min, q.min_size, q.max_size, q.center_x, q.center_z,
+              q.max_results, q.precise_afk)
+    return req
+
+
+class SlimeServer:
+    """The search server of the C ABI (slime_b200_server_*): submit requests, poll or wait for
+    tickets, take results with their submission-to-completion latency."""
+
+    QUEUED, RUNNING, DONE, FAILED, UNKNOWN = 0, 1, 2, -1, -2
+
+    def __init__(self, device_bytes: int = 8 << 30, tiles_per_step: int = 0,
+                 core: SlimeCoreB200 | None = None):
+        self.core = core or SlimeCoreB200()
+        self.lib = self.core.lib
+        self.handle = self.lib.slime_b200_server_create(device_bytes, tiles_per_step)
+        if not self.handle:
+            raise SlimeError("server_create failed: " + self.lib.slime_b200_last_error().decode())
+
+    def submit(self, q) -> int:
+        t = self.lib.slime_b200_server_submit(self.handle, _ptr(_request(q)))
+        if t < 0:
+            raise SlimeError("server_submit: invalid request")
+        return t
+
+    def poll(self, ticket: int) -> int:
+        return self.lib.slime_b200_server_poll(self.handle, ticket)
+
+    def wait(self, ticket: int, timeout_ms: int = 600_000) -> int:
+        return self.lib.slime_b200_server_wait(self.handle, ticket, timeout_ms)
+
+    def take(self, ticket: int, max_results: int):
+        """(total, ranked results, latency ms) of a finished ticket; total -1 if it failed."""
+        buf = np.zeros(max(max_results, 1), dtype=RESULT_DTYPE)
+        lat = C.c_double()
+        total = self.lib.slime_b200_server_take(self.handle, ticket, _ptr(buf), max_results,
+                                                C.byref(lat))
+        if total == -2:
+            raise SlimeError(f"ticket {ticket} is not finished")
+        n = 0 if total < 0 else min(total, max_results)
+        return total, buf[:n].copy(), lat.value
+
+    def close(self):
+        if self.handle:
+            self.lib.slime_b200_server_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
