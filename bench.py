@@ -159,6 +159,136 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
+def run_other(args):
+    """One JSON line for the plain, batch or served workload (one GPU, host API timing)."""
+    import numpy as np
+    import torch
+    torch.cuda.set_device(0)
+    from slime_b200 import build
+    from slime_b200.lib import SlimeCoreB200, SlimeServer
+    build.build()
+    core = SlimeCoreB200()
+    sampler = ClockSampler(0)
+    line = {"n_gpus": 1, "steps": args.steps, "warmup": args.warmup, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "int64", "data": "synthetic"}
+    if args.workload in ("plain", "batch"):
+        if args.workload == "plain":
+            q = workloads.plain_search()
+            work = [q]
+            centres = q.centres
+
+            def run_ours():
+                core.lib.reset_cancel()
+                return [core.search(q.seed, q.radius, q.min_size, q.max_size, q.rd_min, q.center_x,
+                                    q.center_z, q.max_results, 0)]
+        else:
+            work = workloads.batch_searches()
+            centres = sum(q.centres for q in work)
+
+            def run_ours():
+                core.lib.reset_cancel()
+                return core.search_batch(work)
+
+        def run_loop():
+            out = []
+            for q in work:
+                core.lib.reset_cancel()
+                out.append(core.search(q.seed, q.radius, q.min_size, q.max_size, q.rd_min, q.center_x,
+                                       q.center_z, q.max_results, 0))
+            return out
+
+        for _ in range(args.warmup):
+            run_ours()
+            run_loop()
+        torch.cuda.synchronize()
+        sampler.start()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            res = run_ours()
+        t_ours = (time.perf_counter() - t0) / args.steps
+        kms, launches = core.last_search_stats()
+        t0 = time.perf_counter()
+        for _ in range(args.steps):
+            ref = run_loop()
+        t_loop = (time.perf_counter() - t0) / args.steps
+        sampler.stop()
+        assert all(a[0] == b[0] and np.array_equal(a[1], b[1]) for a, b in zip(res, ref))
+        name = ("T centres/s plain 4,001^2 threshold-40 search" if args.workload == "plain"
+                else "T centres/s 64-seed mixed batch")
+        line.update({
+            "metric": name, "value": centres / t_ours / 1e12, "unit": "T centres/s",
+            "ms_per_step": t_ours * 1e3,
+            "e2e": {"value": centres / t_ours / 1e12, "unit": "T centres/s", "h2d_bytes_per_step": 48 * len(work),
+                    "d2h_bytes_per_step": int(sum(min(t, q.max_results) * 24 for (t, _), q in zip(res, work)))},
+            "gpu_launches": launches,
+            "config": {"workload": (f"4,001^2 centres about (0,0), threshold 40, top 100,000, seed {work[0].seed}"
+                                    if args.workload == "plain" else
+                                    "64 seeds: centres uniform in +-1e6, radii log-uniform in [1e3, 2e5], "
+                                    "thresholds uniform in [45, 60], top 1,000 each"),
+                       "centres": centres, "loop_ms_per_step": t_loop * 1e3,
+                       "vs_loop": t_loop / t_ours,
+                       "timing": "host wall clock around the C-ABI calls (inputs and results in host memory)"},
+            "clocks": sampler.summary(),
+        })
+        print(json.dumps(line), flush=True)
+        return
+
+    # served: replay the first N requests of the seeded Poisson stream against the server.
+    stream = workloads.served_stream(args.requests)
+    reqs = [q for _, q in stream]
+    arrivals = [t for t, _ in stream]
+    biome = sum(1 for q in reqs if q.biome_flags)
+    with SlimeServer(core=core) as server:
+        # Capacity: every request submitted at once.
+        sampler.start()
+        t0 = time.perf_counter()
+        tickets = [server.submit(q) for q in reqs]
+        for t in tickets:
+            server.wait(t)
+        makespan = time.perf_counter() - t0
+        for t, q in zip(tickets, reqs):
+            server.take(t, q.max_results)
+        capacity = len(reqs) / makespan
+        # Poisson arrivals at 0.8x that capacity (the stream was drawn at one request per second).
+        scale = 1.0 / (0.8 * capacity)
+        lat = []
+        t0 = time.perf_counter()
+        tickets = []
+        for at, q in zip(arrivals, reqs):
+            delay = at * scale - (time.perf_counter() - t0)
+            if delay > 0:
+                time.sleep(delay)
+            tickets.append(server.submit(q))
+        for t in tickets:
+            server.wait(t)
+        span = time.perf_counter() - t0
+        totals = []
+        for t, q in zip(tickets, reqs):
+            total, _, ms = server.take(t, q.max_results)
+            lat.append(ms)
+            totals.append(total)
+        sampler.stop()
+    lat.sort()
+    centres = sum(q.centres for q in reqs)
+    line.update({
+        "metric": "served requests/s at 0.8x batched capacity", "value": len(reqs) / span, "unit": "requests/s",
+        "ms_per_step": span * 1e3,
+        "latency_ms": {"p50": statistics.median(lat), "p99": lat[min(len(lat) - 1, int(0.99 * len(lat)))],
+                       "max": lat[-1]},
+        "e2e": {"value": len(reqs) / span, "unit": "requests/s", "h2d_bytes_per_step": 48 * len(reqs),
+                "d2h_bytes_per_step": int(sum(min(max(t, 0), q.max_results) * 24 for t, q in zip(totals, reqs)))},
+        "gpu_launches": None,
+        "config": {"workload": f"first {len(reqs)} requests of the 10,000-request stream: centres uniform in "
+                               "+-1.8e6, radii log-uniform in [100, 1,875,000], thresholds uniform in [40, 65]",
+                   "centres": centres, "capacity_requests_per_s": capacity,
+                   "arrival_rate_per_s": 0.8 * capacity, "failed": sum(1 for t in totals if t < 0),
+                   "biome_requests_run_without_exclusion": biome,
+                   "timing": "submission to completion per request, host wall clock"},
+        "clocks": sampler.summary(),
+    })
+    print(json.dumps(line), flush=True)
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -168,10 +298,18 @@ def main():
     ap.add_argument("--radius", type=int, default=workloads.WORLD_RADIUS,
                     help="search radius in chunks (default: the full world)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--workload", default="full_world", choices=["full_world", "plain", "batch", "served"],
+                    help="full_world (the headline), plain (4,001^2 threshold 40), batch (64 mixed "
+                         "seeds), served (Poisson request stream)")
+    ap.add_argument("--requests", type=int, default=60, help="served: requests of the stream replayed")
     args = ap.parse_args()
     rank, local_rank, world = env_rank()
     if args.impl == "reference":
         run_reference(args, rank, world)
+        return
+    if args.workload != "full_world":
+        if rank == 0:
+            run_other(args)
         return
 
     import numpy as np
