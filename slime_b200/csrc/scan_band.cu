@@ -134,13 +134,24 @@ __device__ __forceinline__ uint32_t combo_word(const BandSmem& S, int r, int com
     return S.ring[slot][q][combo >> 1][word] & (S.ring[slot][q][kSwPlane][word] ^ fx);
 }
 
+// Row `r` (0..19) of the union of the 16 windows of a 4x4 centre group, as a 20-bit column mask:
+// columns 8 - h .. 11 + h with h the widest window row that reaches box row r.
+__host__ __device__ constexpr uint32_t group_union_mask(int r) {
+    int h = 0;
+    for (int dz = 0; dz < 4; ++dz)
+        if (r - dz >= 0 && r - dz <= 16 && window_half_width(r - dz) > h) h = window_half_width(r - dz);
+    return ((1u << (2 * h + 4)) - 1u) << (8 - h);
+}
+
 // Exact window counts of the 16 centres of group g of word `word` for one combo, from the 20
-// ring rows of strips st-4..st. Lanes 0..19 fetch one 20-column row slice each; lanes 0..15 then
-// count one centre (dx = lane & 3, dz = lane >> 2) over 17 shuffled slices. Centres in range are
-// appended to the hit list. Warp-uniform arguments; called by the whole warp.
+// ring rows of strips st-4..st. Lanes 0..19 fetch one 20-column row slice each. First the whole
+// union of the 16 windows (332 cells; `umask` = this lane's row of it) is counted with one
+// reduction: below the threshold no window can reach it. Otherwise each lane counts half a window
+// of one centre over shuffled slices. Centres in range are appended to the hit list.
+// Warp-uniform arguments; called by the whole warp.
 template <bool kMasked, bool kIndep>
 __device__ __forceinline__ void exact_group(const BandSmem& S, const BandArgs& a, const Tile& T, int combo,
-                                         uint32_t fx, int word, int g, int st, int lane) {
+                                         uint32_t fx, int word, int g, int st, int lane, uint32_t umask) {
     const int ph = combo_phase<kIndep>(combo), m = combo_band<kIndep>(combo);
     const int c0 = word * 32 + 4 * g;       // first window column (tile-relative input col)
     const int r0 = 4 * (st - 4);            // first window row (tile-relative input row)
@@ -154,6 +165,7 @@ __device__ __forceinline__ void exact_group(const BandSmem& S, const BandArgs& a
         }
         slice = __funnelshift_r(lo, hi, 4 * g) & 0xFFFFFu;
     }
+    if ((int)__reduce_add_sync(kFull, (unsigned)__popc(slice & umask)) < a.min_size) return;
     // Lane l counts window rows 0..8 (l < 16) or 9..16 (l >= 16) of centre l % 16; the halves
     // are then added across the two half-warps.
     const int dx = lane & 3, dz = (lane >> 2) & 3, half = lane >> 4;
@@ -209,7 +221,7 @@ struct Counter {
 template <bool kMasked, bool kIndep>
 __device__ __forceinline__ void second_test(const BandSmem& S, const BandArgs& a, const Tile& T, uint32_t flag,
                                             uint32_t re, uint32_t ro, uint32_t n23, uint32_t cm, uint32_t fx,
-                                            uint32_t thr4, int combo, int lane, int st) {
+                                            uint32_t thr4, int combo, int lane, int st, uint32_t umask) {
     const int r0 = 4 * (st - 4);  // rows 0 and 1 of strip st - 4
     uint32_t w0 = combo_word<kIndep>(S, r0, combo, fx, lane), w1 = combo_word<kIndep>(S, r0 + 1, combo, fx, lane);
     if (kMasked) { w0 &= cm; w1 &= cm; }
@@ -230,7 +242,7 @@ __device__ __forceinline__ void second_test(const BandSmem& S, const BandArgs& a
     for (unsigned todo = __ballot_sync(kFull, gm != 0); todo; todo &= todo - 1) {
         const int word = __ffs(todo) - 1;
         for (uint32_t gw = __shfl_sync(kFull, gm, word); gw; gw &= gw - 1)
-            exact_group<kMasked, kIndep>(S, a, T, combo, fx, word, __ffs(gw) - 1, st, lane);
+            exact_group<kMasked, kIndep>(S, a, T, combo, fx, word, __ffs(gw) - 1, st, lane, umask);
     }
 }
 
@@ -242,7 +254,7 @@ __device__ __forceinline__ void second_test(const BandSmem& S, const BandArgs& a
 template <bool kMasked, bool kIndep>
 __device__ __forceinline__ void count_strip(BandSmem& S, const BandArgs& a, const Tile& T, Counter& C,
                                             int slot, int t, int st, int warp, int lane, uint32_t fx,
-                                            uint32_t lastmask, uint32_t thr4, uint32_t& guard) {
+                                            uint32_t lastmask, uint32_t thr4, uint32_t umask, uint32_t& guard) {
     const int r0 = 4 * t;  // t is a compile-time constant after unrolling
     const int hs = st % 5;
     const uint32_t live = st >= 4 ? lastmask : 0u;  // boxes are complete from the fifth strip on
@@ -290,7 +302,7 @@ __device__ __forceinline__ void count_strip(BandSmem& S, const BandArgs& a, cons
         for (int k = 0; k < kUsed; ++k)
             if (__any_sync(kFull, fl[k] != 0))
                 second_test<kMasked, kIndep>(S, a, T, fl[k], C.re[k], C.ro[k], n23s[k], kMasked ? C.cm[k] : ~0u,
-                                             fx, thr4, warp + kWarps * k, lane, st);
+                                             fx, thr4, warp + kWarps * k, lane, st, umask);
     }
 }
 
@@ -331,6 +343,7 @@ __device__ __forceinline__ bool band_tile(BandSmem& S, const BandArgs& a, int64_
     // (groups 4..7 of word 31 hold centres 1,008+ of the tile, which belong to the next tile).
     const uint32_t fx = ((warp ^ (warp >> 1)) & 1) ? 0u : ~0u;
     const uint32_t lastmask = lane == kWords - 1 ? 0x0000C0C0u : ~0u;
+    const uint32_t umask = lane < 20 ? group_union_mask(lane) : 0u;
     uint32_t guard = 0;
     {
         Tile T;
@@ -495,9 +508,9 @@ __device__ __forceinline__ bool band_tile(BandSmem& S, const BandArgs& a, int64_
 #pragma unroll
             for (int t = 0; t < 2; ++t) {
                 if (interior)
-                    count_strip<false, kIndep>(S, a, T, C, slot, t, 2 * b + t, warp, lane, fx, lastmask, thr4, guard);
+                    count_strip<false, kIndep>(S, a, T, C, slot, t, 2 * b + t, warp, lane, fx, lastmask, thr4, umask, guard);
                 else
-                    count_strip<true, kIndep>(S, a, T, C, slot, t, 2 * b + t, warp, lane, fx, lastmask, thr4, guard);
+                    count_strip<true, kIndep>(S, a, T, C, slot, t, 2 * b + t, warp, lane, fx, lastmask, thr4, umask, guard);
             }
         }
         __syncthreads();  // the next tile reuses ring slots and histories still read above
