@@ -126,6 +126,17 @@ int64_t slime_b200_last_rare_chunks(void);
  * bands) for the last search. */
 void slime_b200_set_engine(int32_t mode, int32_t band_min_threshold);
 
+/* The automatic engine rule as 6 numbers: {band_min_threshold, band_min_periods,
+ * band_fast_threshold, band_fast_periods, indep_min_threshold, indep_min_centres}. The
+ * shared-LCG band engine takes areas at least band_min_periods x 2^17 chunks wide from
+ * band_min_threshold, or band_fast_periods x 2^17 wide from band_fast_threshold; independent bands
+ * take areas of indep_min_centres centres or more from indep_min_threshold; the general scan
+ * takes the rest. Thresholds 28..222 (222 disables a branch), periods 2..64. Returns 0, or -1
+ * for a wrong count or a value out of range (nothing is changed). slime_b200/autotune.py measures
+ * the crossovers on the local GPU and writes them; the defaults are B200 measurements. */
+int32_t slime_b200_set_engine_rule(const int64_t* rule, int32_t n);
+int32_t slime_b200_get_engine_rule(int64_t* rule, int32_t n);
+
 /* Generator variant of the band engine (results are identical): band_mad_add != 0 issues the
  * per-band add on the multiply pipe instead of the integer ALU. */
 void slime_b200_set_tuning(int32_t band_mad_add);

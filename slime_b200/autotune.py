@@ -1,0 +1,143 @@
+"""Measure the engine crossovers of the slime-chunk search on the local GPU and write the rule.
+
+    python -m slime_b200.autotune [--out slime_b200/tuning_b200.json] [--quick]
+
+For each (radius, threshold) point of a grid the search is timed with every engine that applies
+(the general scan, independent bands, and the shared-LCG band engine where the area spans two
+periods), forced through slime_b200_set_engine; every engine must return the same total and the
+same ranked sites. From the timings it derives the six numbers of slime_b200_set_engine_rule:
+
+  band_min_threshold, band_min_periods   shared LCG from this threshold on areas this many
+  band_fast_threshold, band_fast_periods 2^17-chunk periods wide (two branches of the rule)
+  indep_min_threshold, indep_min_centres independent bands instead of the general scan
+
+and writes them with the raw timings to a JSON file. SlimeCoreB200 applies that file when it
+loads the library. The general scan's rate does not depend on the area once it fills the GPU, so
+it is timed on the smaller areas only and extrapolated to the larger ones.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes
+import json
+import time
+from pathlib import Path
+
+import numpy as np
+
+PERIOD = 1 << 17
+DEFAULT_OUT = Path(__file__).with_name("tuning_b200.json")
+SEED = 0x5EED_B200  # any world seed: rates do not depend on it
+
+
+def _time(core, mode, radius, thr, reps=2):
+    core.lib.slime_b200_set_engine(mode, 0)
+    best, out = None, None
+    for _ in range(reps):
+        core.lib.reset_cancel()
+        t = time.perf_counter()
+        out = core.search(SEED, radius, thr, 221, 0, 0, 0, 200)
+        dt = time.perf_counter() - t
+        best = dt if best is None else min(best, dt)
+    return best, out
+
+
+def measure(core, quick=False):
+    radii = [30_000, 100_000, 300_000, 600_000] + ([] if quick else [1_000_000])
+    rows = []
+    general_rate = {}
+    for r in radii:
+        w = 2 * r + 1
+        for thr in range(40, 62, 4 if quick else 2):
+            if r >= 300_000 and thr < 44:
+                continue  # hours of band work for no decision: the general scan wins there
+            point = {"radius": r, "threshold": thr, "centres": w * w}
+            ref = None
+            engines = [("indep", 3)] + ([("band", 2)] if w >= 2 * PERIOD else [])
+            if r <= 100_000:
+                engines.insert(0, ("general", 1))
+            for name, mode in engines:
+                dt, out = _time(core, mode, r, thr, reps=1 if r >= 600_000 else 2)
+                if ref is None:
+                    ref = out
+                elif out[0] != ref[0] or not np.array_equal(out[1], ref[1]):
+                    raise RuntimeError(f"engines disagree at radius {r} threshold {thr}")
+                point[name + "_s"] = dt
+            if "general_s" in point:
+                general_rate[thr] = point["centres"] / point["general_s"]
+            else:
+                point["general_s"] = point["centres"] / general_rate.get(thr, min(general_rate.values()))
+            rows.append(point)
+    core.lib.slime_b200_set_engine(0, 0)
+    return rows
+
+
+def derive(rows):
+    """The six rule numbers from the timings. Independent bands take a threshold when they beat
+    the general scan there and at every higher measured threshold of the area. The two
+    shared-LCG branches are chosen among the measured (threshold, periods) crossovers as the pair
+    whose rule costs least over the whole grid (sum of each point's time over its best time)."""
+    def min_winning_thr(pts, a, b):
+        pts = sorted(pts, key=lambda p: p["threshold"])
+        best = 222
+        for p in reversed(pts):
+            if a in p and b in p and p[a] < p[b]:
+                best = p["threshold"]
+            else:
+                break
+        return best
+
+    by_r = {}
+    for p in rows:
+        by_r.setdefault(p["radius"], []).append(p)
+    indep_thr = {r: min_winning_thr(pts, "indep_s", "general_s") for r, pts in by_r.items()}
+    indep_min_threshold = max(indep_thr.values())
+    wins = [r for r, t in indep_thr.items() if t <= indep_min_threshold]
+    indep_min_centres = (2 * min(wins) + 1) ** 2 if wins else 1 << 62
+    band_thr = {r: min_winning_thr(pts, "band_s", "indep_s") for r, pts in by_r.items()
+                if any("band_s" in p for p in pts)}
+    cands = sorted({(t, (2 * r + 1) // PERIOD) for r, t in band_thr.items()} | {(222, 64)})
+
+    def cost(a, b):
+        total = 0.0
+        for p in rows:
+            w = 2 * p["radius"] + 1
+            best = min(p[k] for k in ("general_s", "indep_s", "band_s") if k in p)
+            thr = p["threshold"]
+            if "band_s" in p and any(thr >= t and w >= n * PERIOD for t, n in (a, b)):
+                t_rule = p["band_s"]
+            elif w * w >= indep_min_centres and thr >= indep_min_threshold:
+                t_rule = p["indep_s"]
+            else:
+                t_rule = p["general_s"]
+            total += t_rule / best
+        return total
+
+    a, b = min(((x, y) for x in cands for y in cands), key=lambda ab: cost(*ab))
+    return [a[0], max(2, a[1]), b[0], max(2, b[1]), indep_min_threshold, indep_min_centres]
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--out", default=str(DEFAULT_OUT))
+    ap.add_argument("--quick", action="store_true", help="coarser grid (threshold step 4, no 1M radius)")
+    ap.add_argument("--rederive", action="store_true", help="recompute the rule from the file's timings")
+    args = ap.parse_args()
+    from slime_b200 import build
+    from slime_b200.lib import SlimeCoreB200
+    build.build()
+    core = SlimeCoreB200(apply_tuning=False)
+    name = ctypes.create_string_buffer(256)
+    core.lib.get_cuda_device_name(name, 256)
+    rows = measure(core, quick=args.quick) if not args.rederive else json.loads(Path(args.out).read_text())["points"]
+    rule = derive(rows)
+    doc = {"device": name.value.decode(errors="replace"),
+           "rule": dict(zip(["band_min_threshold", "band_min_periods", "band_fast_threshold",
+                             "band_fast_periods", "indep_min_threshold", "indep_min_centres"], rule)),
+           "seed": SEED, "max_results": 200, "points": rows}
+    Path(args.out).write_text(json.dumps(doc, indent=1) + "\n")
+    print(json.dumps(doc["rule"]))
+
+
+if __name__ == "__main__":
+    main()

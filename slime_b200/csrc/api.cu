@@ -555,6 +555,36 @@ void slime_b200_set_engine(int32_t mode, int32_t band_min_threshold) {
 
 const char* slime_b200_last_error(void) { return ctx().last_error.c_str(); }
 
+int32_t slime_b200_set_engine_rule(const int64_t* rule, int32_t n) {
+    if (!rule || n != 6) return -1;
+    const int64_t bt = rule[0], bp = rule[1], ft = rule[2], fp = rule[3], it = rule[4], ic = rule[5];
+    if (bt < 28 || bt > 222 || ft < 28 || ft > 222 || it < 28 || it > 222 || bp < 2 || bp > 64 ||
+        fp < 2 || fp > 64 || ic < 0)
+        return -1;
+    std::lock_guard<std::mutex> lock(ctx().mu);
+    slime::Context& c = ctx();
+    c.band_min_threshold = (int32_t)bt;
+    c.band_min_periods = (int32_t)bp;
+    c.band_fast_threshold = (int32_t)ft;
+    c.band_fast_periods = (int32_t)fp;
+    c.indep_min_threshold = (int32_t)it;
+    c.indep_min_centres = ic;
+    return 0;
+}
+
+int32_t slime_b200_get_engine_rule(int64_t* rule, int32_t n) {
+    if (!rule || n != 6) return -1;
+    std::lock_guard<std::mutex> lock(ctx().mu);
+    const slime::Context& c = ctx();
+    rule[0] = c.band_min_threshold;
+    rule[1] = c.band_min_periods;
+    rule[2] = c.band_fast_threshold;
+    rule[3] = c.band_fast_periods;
+    rule[4] = c.indep_min_threshold;
+    rule[5] = c.indep_min_centres;
+    return 0;
+}
+
 int32_t slime_b200_search_batch(const SlimeBatchRequest* requests, int32_t n, ExtChunkResult* results,
                                 int64_t* totals) {
     std::lock_guard<std::mutex> lock(ctx().mu);

@@ -42,13 +42,12 @@ int32_t Context::engine_for(const SearchSpec& q) const {
     if (engine_override == 1 || q.min_size < 28) return kAlgoGeneral;
     if (engine_override == 2) return kAlgoBand;
     if (engine_override == 3) return kAlgoIndep;
-    // Measured on B200 (T centres/s, shared band / independent bands): radius 140k thr 50 0.49 /
-    // 1.02, thr 60 1.09 / 1.44; radius 300k thr 50 0.76 / 1.00, thr 60 1.84 / -; radius 600k thr
-    // 48 0.71 / 0.85, thr 50 1.17 / 1.09, thr 52 1.75 / 1.28, thr 55 2.56 / 1.43, thr 60 3.27 /
-    // 1.52. The shared LCG pays off with many periods (its work is shared by every band and
-    // phase pair) and a high threshold.
+    // The rule's numbers are measured crossovers (slime_b200/autotune.py writes them; the
+    // defaults are the B200 values). The shared LCG pays off with many periods (its work is
+    // shared by every band and phase pair) and a high threshold.
     const int64_t w = 2 * q.rd_max + 1;
-    if (q.min_size >= band_min_threshold && (w >= 7 * kP || (w >= 4 * kP && q.min_size >= 56)))
+    if ((q.min_size >= band_min_threshold && w >= (int64_t)band_min_periods * kP) ||
+        (q.min_size >= band_fast_threshold && w >= (int64_t)band_fast_periods * kP))
         return kAlgoBand;
     if (w * w >= indep_min_centres && q.min_size >= indep_min_threshold) return kAlgoIndep;
     return kAlgoGeneral;

@@ -109,14 +109,17 @@ struct Context {
     DeviceBuffer<int64_t> bt_prefix;
     bool band_ready = false;
     int32_t engine_override = 0;       // 0 auto, 1 general scan, 2 band engine, 3 independent bands
-    // Auto mode uses the shared-LCG band engine from this threshold: below it the exact counts of
-    // the many surviving 4x4 groups dominate and independent bands are faster (B200 crossover
-    // between 48 and 50 on a 1,200,001^2 area).
+    // Engine rule (engine_for; slime_b200_set_engine_rule): the shared-LCG band engine for areas
+    // at least band_min_periods periods wide from band_min_threshold, or band_fast_periods wide
+    // from band_fast_threshold; independent bands for areas of indep_min_centres centres or more
+    // from indep_min_threshold; the general scan otherwise. Defaults: the rule slime_b200/
+    // autotune.py derived on B200 (slime_b200/tuning_b200.json).
     int32_t band_min_threshold = 50;
-    // Auto mode uses the independent-band engine for areas of at least this many centres from
-    // this threshold on.
+    int32_t band_min_periods = 9;
+    int32_t band_fast_threshold = 54;
+    int32_t band_fast_periods = 4;
     int32_t indep_min_threshold = 44;
-    int64_t indep_min_centres = 1000000000;
+    int64_t indep_min_centres = 3600120001;
     int64_t last_rare = 0;             // rare redraw chunks found by the last band search
     int64_t band_fallbacks = 0;        // band searches redone by the general scan
     int32_t band_mad_add = 1;          // generator variant: band adds on the multiply pipe

@@ -57,6 +57,8 @@ SIGNATURES = {
     "slime_b200_microbench": (i32, [i32, i32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "slime_b200_search_noalloc": (i64, [i64, i64, i32, i32, i64, i32, i32, vp, i32]),
     "slime_b200_search_batch": (i32, [vp, i32, vp, vp]),
+    "slime_b200_set_engine_rule": (i32, [vp, i32]),
+    "slime_b200_get_engine_rule": (i32, [vp, i32]),
     "slime_b200_server_create": (vp, [i64, i32]),
     "slime_b200_server_submit": (i64, [vp, vp]),
     "slime_b200_server_poll": (i32, [vp, i64]),
@@ -93,11 +95,29 @@ class SlimeError(RuntimeError):
     pass
 
 
-class SlimeCoreB200:
-    """Pythonic view of the C ABI; every call goes through the exported C functions."""
+TUNING = Path(__file__).with_name("tuning_b200.json")
+RULE_KEYS = ("band_min_threshold", "band_min_periods", "band_fast_threshold", "band_fast_periods",
+             "indep_min_threshold", "indep_min_centres")
 
-    def __init__(self, path: Path | str = LIB):
+
+class SlimeCoreB200:
+    """Pythonic view of the C ABI; every call goes through the exported C functions. The engine
+    rule measured by slime_b200/autotune.py (tuning_b200.json) is applied when present."""
+
+    def __init__(self, path: Path | str = LIB, apply_tuning: bool = True):
         self.lib = load(path)
+        if apply_tuning and TUNING.exists():
+            import json
+            self.set_engine_rule(json.loads(TUNING.read_text())["rule"])
+
+    def set_engine_rule(self, rule: dict):
+        vals = np.array([int(rule[k]) for k in RULE_KEYS], dtype=np.int64)
+        self._check(self.lib.slime_b200_set_engine_rule(_ptr(vals), len(vals)) == 0, "set_engine_rule")
+
+    def engine_rule(self) -> dict:
+        vals = np.zeros(len(RULE_KEYS), dtype=np.int64)
+        self._check(self.lib.slime_b200_get_engine_rule(_ptr(vals), len(vals)) == 0, "get_engine_rule")
+        return dict(zip(RULE_KEYS, (int(v) for v in vals)))
 
     def _check(self, ok: bool, what: str):
         if not ok:

@@ -75,3 +75,30 @@ def test_invalid_arguments_rejected_before_device(lib):
     assert lib.search_slime_clusters_gpu_v1_centered(1, 10, 40, 221, 0, 0, 0, p, 0, 0) == -1
     assert lib.search_slime_clusters_gpu_v1_centered(1, (2**31 - 1 - 19) // 2 + 1, 40, 221, 0, 0, 0, p, 4, 0) == -1
     assert lib.search_slime_clusters_gpu_v1_centered(1, 100, 40, 221, 0, 2**31 - 100, 0, p, 4, 0) == -1
+
+
+def test_engine_rule_round_trip_and_range_checks(lib):
+    from slime_b200.lib import RULE_KEYS, SlimeCoreB200
+    core = SlimeCoreB200(apply_tuning=False)
+    before = core.engine_rule()
+    assert set(before) == set(RULE_KEYS)
+    try:
+        rule = dict(before, band_min_threshold=52, band_fast_periods=5, indep_min_centres=123)
+        core.set_engine_rule(rule)
+        assert core.engine_rule() == rule
+        bad = np.array([27, 7, 56, 4, 44, 10], dtype=np.int64)  # threshold below the band range
+        assert lib.slime_b200_set_engine_rule(bad.ctypes.data_as(ctypes.c_void_p), 6) == -1
+        assert lib.slime_b200_set_engine_rule(bad.ctypes.data_as(ctypes.c_void_p), 5) == -1
+        assert core.engine_rule() == rule
+    finally:
+        core.set_engine_rule(before)
+
+
+def test_committed_tuning_file_is_a_valid_rule():
+    import json
+    from slime_b200.lib import RULE_KEYS, TUNING
+    doc = json.loads(TUNING.read_text())
+    assert set(doc["rule"]) == set(RULE_KEYS)
+    assert 28 <= doc["rule"]["band_min_threshold"] <= 222 and doc["points"]
+    for p in doc["points"]:
+        assert p["indep_s"] > 0 and p["general_s"] > 0
