@@ -54,6 +54,7 @@ template <bool kIndep>
 constexpr int row_words() { return kIndep ? kRowWordsI : kRowWords; }
 
 constexpr int kBatchRows = 8;               // rows per barrier: two 4-row strips
+constexpr int kCandCap = 64;                // per warp: groups waiting for their union count
 constexpr int kRingSlots = 4;               // batches b-2..b are read while b+1 is generated
 
 struct __align__(16) BandSmem {
@@ -62,6 +63,7 @@ struct __align__(16) BandSmem {
     uint32_t hist_o[5][kMaxCombos][kWords];   // (odd groups)
     uint32_t rows[3][kBatchRows * kRowWordsI];  // row terms of 3 batches, filled by bulk copies
     unsigned long long rows_bar[3];           // mbarriers of the three row-term buffers
+    uint32_t cand[kWarps][kCandCap];          // per warp: combo << 24 | word << 19 | group << 16 | strip
     BandArgs args;                            // batched kernel: the current tile's search
     long long next_tile;                      // batched kernel: tile taken from the queue
     int search;                               // batched kernel: its search
@@ -218,10 +220,49 @@ struct Counter {
 // outer cells of rows 0, 1 (strip st - 4) and of rows 18, 19 (strip st), which no window of the
 // group reaches, are removed from the box (368 cells remain; the box bytes are exact, so no byte
 // borrows). Survivors are counted exactly. Called by the whole warp.
+// The union counts of the warp's candidate groups, 32 at a time (lane = group), then the exact
+// counts of those that reach the threshold. Called by the whole warp; the caller empties the list.
 template <bool kMasked, bool kIndep>
-__device__ __forceinline__ void second_test(const BandSmem& S, const BandArgs& a, const Tile& T, uint32_t flag,
+__device__ __forceinline__ void flush_cands(BandSmem& S, const BandArgs& a, const Tile& T, uint32_t fx, int warp,
+                                         int lane, uint32_t umask, int ncand) {
+    __syncwarp();
+    for (int base = 0; base < ncand; base += 32) {
+        const int j = base + lane;
+        uint32_t e = 0;
+        bool pass = false;
+        if (j < ncand) {
+            e = S.cand[warp][j];
+            const int combo = (int)(e >> 24), word = (int)((e >> 19) & 31), g = (int)((e >> 16) & 7);
+            const int r0 = 4 * ((int)(e & 0xFFFF) - 4);
+            uint32_t cml = ~0u, cmh = word + 1 < kWords ? ~0u : 0u;
+            if (kMasked) {
+                cml = column_mask(a, T, word, combo_phase<kIndep>(combo));
+                cmh &= word + 1 < kWords ? column_mask(a, T, word + 1, combo_phase<kIndep>(combo)) : 0u;
+            }
+            const int wh = min(word + 1, kWords - 1);
+            int sum = 0;
+#pragma unroll
+            for (int r = 0; r < 20; ++r) {
+                const uint32_t lo = combo_word<kIndep>(S, r0 + r, combo, fx, word) & cml;
+                const uint32_t hi = combo_word<kIndep>(S, r0 + r, combo, fx, wh) & cmh;
+                sum += __popc(__funnelshift_r(lo, hi, 4 * g) & group_union_mask(r));
+            }
+            pass = sum >= a.min_size;
+        }
+        for (unsigned pm = __ballot_sync(kFull, pass); pm; pm &= pm - 1) {
+            const uint32_t ee = __shfl_sync(kFull, e, __ffs(pm) - 1);
+            exact_group<kMasked, kIndep>(S, a, T, (int)(ee >> 24), fx, (int)((ee >> 19) & 31), (int)((ee >> 16) & 7),
+                                         (int)(ee & 0xFFFF), lane, umask);
+        }
+    }
+    __syncwarp();
+}
+
+template <bool kMasked, bool kIndep, bool kCands>
+__device__ __forceinline__ void second_test(BandSmem& S, const BandArgs& a, const Tile& T, uint32_t flag,
                                             uint32_t re, uint32_t ro, uint32_t n23, uint32_t cm, uint32_t fx,
-                                            uint32_t thr4, int combo, int lane, int st, uint32_t umask) {
+                                            uint32_t thr4, int combo, int lane, int st, uint32_t umask, int warp,
+                                            int& ncand) {
     const int r0 = 4 * (st - 4);  // rows 0 and 1 of strip st - 4
     uint32_t w0 = combo_word<kIndep>(S, r0, combo, fx, lane), w1 = combo_word<kIndep>(S, r0 + 1, combo, fx, lane);
     if (kMasked) { w0 &= cm; w1 &= cm; }
@@ -239,11 +280,43 @@ __device__ __forceinline__ void second_test(const BandSmem& S, const BandArgs& a
         const int bit = __ffs(f) - 1;
         gm |= 1u << (2 * (bit >> 3) + 7 - (bit & 7));
     }
-    for (unsigned todo = __ballot_sync(kFull, gm != 0); todo; todo &= todo - 1) {
-        const int word = __ffs(todo) - 1;
-        for (uint32_t gw = __shfl_sync(kFull, gm, word); gw; gw &= gw - 1)
-            exact_group<kMasked, kIndep>(S, a, T, combo, fx, word, __ffs(gw) - 1, st, lane, umask);
+    if (!kCands) {  // few survivors (high thresholds): count each group at once
+        for (unsigned todo = __ballot_sync(kFull, gm != 0); todo; todo &= todo - 1) {
+            const int word = __ffs(todo) - 1;
+            for (uint32_t gw = __shfl_sync(kFull, gm, word); gw; gw &= gw - 1)
+                exact_group<kMasked, kIndep>(S, a, T, combo, fx, word, __ffs(gw) - 1, st, lane, umask);
+        }
+        return;
     }
+    // Survivors join the warp's candidate list (lane order, groups ascending); the list is
+    // counted at the end of the batch, or now when it would overflow.
+    const int n = __popc(gm);
+    int pos = n;  // inclusive prefix sum over lanes
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const int v = __shfl_up_sync(kFull, pos, d);
+        if (lane >= d) pos += v;
+    }
+    const int total = __shfl_sync(kFull, pos, 31);
+    if (total == 0) return;
+    if (total > kCandCap) {  // a dense word set (low threshold): count this combo's groups now
+        for (unsigned todo = __ballot_sync(kFull, gm != 0); todo; todo &= todo - 1) {
+            const int word = __ffs(todo) - 1;
+            for (uint32_t gw = __shfl_sync(kFull, gm, word); gw; gw &= gw - 1)
+                exact_group<kMasked, kIndep>(S, a, T, combo, fx, word, __ffs(gw) - 1, st, lane, umask);
+        }
+        return;
+    }
+    if (ncand + total > kCandCap) {
+        flush_cands<kMasked, kIndep>(S, a, T, fx, warp, lane, umask, ncand);
+        ncand = 0;
+    }
+    int idx = ncand + pos - n;
+    for (uint32_t gw = gm; gw; gw &= gw - 1)
+        S.cand[warp][idx++] = ((uint32_t)combo << 24) | ((uint32_t)lane << 19) | ((uint32_t)(__ffs(gw) - 1) << 16) |
+                              (uint32_t)st;
+    ncand += total;
+    __syncwarp();
 }
 
 // Counts one 4-row strip (rows 4t..4t+3 of ring slot `slot`) for the warp's four combo slots as
@@ -251,10 +324,11 @@ __device__ __forceinline__ void second_test(const BandSmem& S, const BandArgs& a
 // threshold test. Only when a lane flags a group does the warp take the second test. With the
 // shared LCG, slots of combos beyond the launch's band count read zero planes and never flag;
 // independent bands use two slots per warp (32 combos) and skip combos beyond the band count.
-template <bool kMasked, bool kIndep>
+template <bool kMasked, bool kIndep, bool kCands>
 __device__ __forceinline__ void count_strip(BandSmem& S, const BandArgs& a, const Tile& T, Counter& C,
                                             int slot, int t, int st, int warp, int lane, uint32_t fx,
-                                            uint32_t lastmask, uint32_t thr4, uint32_t umask, uint32_t& guard) {
+                                            uint32_t lastmask, uint32_t thr4, uint32_t umask, uint32_t& guard,
+                                            int& ncand) {
     const int r0 = 4 * t;  // t is a compile-time constant after unrolling
     const int hs = st % 5;
     const uint32_t live = st >= 4 ? lastmask : 0u;  // boxes are complete from the fifth strip on
@@ -301,8 +375,8 @@ __device__ __forceinline__ void count_strip(BandSmem& S, const BandArgs& a, cons
 #pragma unroll
         for (int k = 0; k < kUsed; ++k)
             if (__any_sync(kFull, fl[k] != 0))
-                second_test<kMasked, kIndep>(S, a, T, fl[k], C.re[k], C.ro[k], n23s[k], kMasked ? C.cm[k] : ~0u,
-                                             fx, thr4, warp + kWarps * k, lane, st, umask);
+                second_test<kMasked, kIndep, kCands>(S, a, T, fl[k], C.re[k], C.ro[k], n23s[k], kMasked ? C.cm[k] : ~0u,
+                                             fx, thr4, warp + kWarps * k, lane, st, umask, warp, ncand);
     }
 }
 
@@ -333,7 +407,7 @@ __device__ __forceinline__ void band_cta_init(BandSmem& S, int tid) {
 
 // One tile of one search (block-uniform arguments; all threads). Returns false when a bounded
 // wait gave up (the search's overflow word gets bit 4 and the CTA must stop).
-template <bool kMadAdd, bool kIndep>
+template <bool kMadAdd, bool kIndep, bool kCands>
 __device__ __forceinline__ bool band_tile(BandSmem& S, const BandArgs& a, int64_t tile, int tid, int lane,
                                           int warp, uint32_t& bar_phase) {
     const int nb = a.nb;
@@ -345,6 +419,7 @@ __device__ __forceinline__ bool band_tile(BandSmem& S, const BandArgs& a, int64_
     const uint32_t lastmask = lane == kWords - 1 ? 0x0000C0C0u : ~0u;
     const uint32_t umask = lane < 20 ? group_union_mask(lane) : 0u;
     uint32_t guard = 0;
+    int ncand = 0;  // warp-uniform length of this warp's candidate list
     {
         Tile T;
         const int ut = (int)(tile % a.u_tiles);
@@ -508,9 +583,18 @@ __device__ __forceinline__ bool band_tile(BandSmem& S, const BandArgs& a, int64_
 #pragma unroll
             for (int t = 0; t < 2; ++t) {
                 if (interior)
-                    count_strip<false, kIndep>(S, a, T, C, slot, t, 2 * b + t, warp, lane, fx, lastmask, thr4, umask, guard);
+                    count_strip<false, kIndep, kCands>(S, a, T, C, slot, t, 2 * b + t, warp, lane, fx, lastmask, thr4, umask,
+                                                       guard, ncand);
                 else
-                    count_strip<true, kIndep>(S, a, T, C, slot, t, 2 * b + t, warp, lane, fx, lastmask, thr4, umask, guard);
+                    count_strip<true, kIndep, kCands>(S, a, T, C, slot, t, 2 * b + t, warp, lane, fx, lastmask, thr4, umask,
+                                                      guard, ncand);
+            }
+            // Candidates of this batch need rows of batches b-2..b, which stay in the ring until
+            // batch b+2 is generated (after the next barrier).
+            if (kCands && ncand) {
+                if (interior) flush_cands<false, kIndep>(S, a, T, fx, warp, lane, umask, ncand);
+                else flush_cands<true, kIndep>(S, a, T, fx, warp, lane, umask, ncand);
+                ncand = 0;
             }
         }
         __syncthreads();  // the next tile reuses ring slots and histories still read above
@@ -520,7 +604,11 @@ __device__ __forceinline__ bool band_tile(BandSmem& S, const BandArgs& a, int64_
     return true;
 }
 
-template <bool kMadAdd, bool kIndep>
+// Survivor handling: below this threshold the 368-cell survivors are many, and batching their
+// union counts per warp (kCands) pays; above it they are rare and are counted at once.
+constexpr int kCandThreshold = 56;
+
+template <bool kMadAdd, bool kIndep, bool kCands>
 __global__ void __launch_bounds__(kTpb, 1) band_scan_kernel(const BandArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     BandSmem& S = *reinterpret_cast<BandSmem*>(smem_raw);
@@ -529,7 +617,7 @@ __global__ void __launch_bounds__(kTpb, 1) band_scan_kernel(const BandArgs a) {
     uint32_t bar_phase = 0;  // bit r: parity of the next completion of rows_bar[r]
     band_cta_init(S, tid);
     for (int64_t tile = a.tile_begin + blockIdx.x; tile < a.tile_end; tile += gridDim.x)
-        if (!band_tile<kMadAdd, kIndep>(S, a, tile, tid, lane, warp, bar_phase)) return;
+        if (!band_tile<kMadAdd, kIndep, kCands>(S, a, tile, tid, lane, warp, bar_phase)) return;
 }
 
 // Many searches in one persistent launch (each search independent-band or shared-LCG): each CTA
@@ -569,7 +657,7 @@ __global__ void __launch_bounds__(kTpb, 1) band_batch_kernel(const BandArgs* arg
         __syncthreads();
         bool ok;
         if (S.args.indep) {
-            ok = band_tile<kMadAdd, true>(S, S.args, S.args.tile_begin + t - prefix[s], tid, lane, warp, bar_phase);
+            ok = band_tile<kMadAdd, true, true>(S, S.args, S.args.tile_begin + t - prefix[s], tid, lane, warp, bar_phase);
         } else {
             // The shared-LCG counter reads every plane: clear planes of bands this search does
             // not generate (a previous search may have left bits there).
@@ -581,7 +669,7 @@ __global__ void __launch_bounds__(kTpb, 1) band_batch_kernel(const BandArgs* arg
                 }
             }
             __syncthreads();
-            ok = band_tile<kMadAdd, false>(S, S.args, S.args.tile_begin + t - prefix[s], tid, lane, warp, bar_phase);
+            ok = band_tile<kMadAdd, false, true>(S, S.args, S.args.tile_begin + t - prefix[s], tid, lane, warp, bar_phase);
         }
         if (!ok) {
             if (tid == 0) atomicOr(S.args.overflow, 4u);
@@ -646,13 +734,19 @@ size_t band_smem_bytes() { return sizeof(BandSmem); }
 int band_tile_out_w() { return kOutW; }
 int band_max_bands() { return kMaxBands; }
 
+template <bool kMadAdd, bool kIndep, bool kCands>
+cudaError_t prepare_one(int bytes) {
+    return cudaFuncSetAttribute(band_scan_kernel<kMadAdd, kIndep, kCands>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                bytes);
+}
+
 cudaError_t band_prepare() {
     const int bytes = (int)sizeof(BandSmem);
     cudaError_t e;
-    if ((e = cudaFuncSetAttribute(band_scan_kernel<false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess ||
-        (e = cudaFuncSetAttribute(band_scan_kernel<true, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess ||
-        (e = cudaFuncSetAttribute(band_scan_kernel<false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess ||
-        (e = cudaFuncSetAttribute(band_scan_kernel<true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess ||
+    if ((e = prepare_one<false, false, false>(bytes)) != cudaSuccess || (e = prepare_one<true, false, false>(bytes)) != cudaSuccess ||
+        (e = prepare_one<false, true, false>(bytes)) != cudaSuccess || (e = prepare_one<true, true, false>(bytes)) != cudaSuccess ||
+        (e = prepare_one<false, false, true>(bytes)) != cudaSuccess || (e = prepare_one<true, false, true>(bytes)) != cudaSuccess ||
+        (e = prepare_one<false, true, true>(bytes)) != cudaSuccess || (e = prepare_one<true, true, true>(bytes)) != cudaSuccess ||
         (e = cudaFuncSetAttribute(band_batch_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess)
         return e;
     return cudaFuncSetAttribute(band_batch_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
@@ -668,12 +762,17 @@ cudaError_t launch_band_batch(const BandArgs* args, const int64_t* prefix, int32
 
 cudaError_t launch_band_scan(const BandArgs& a, int grid, cudaStream_t s) {
     const size_t bytes = sizeof(BandSmem);
-    if (a.indep) {
-        if (a.mad_add) band_scan_kernel<true, true><<<grid, kTpb, bytes, s>>>(a);
-        else band_scan_kernel<false, true><<<grid, kTpb, bytes, s>>>(a);
-    } else {
-        if (a.mad_add) band_scan_kernel<true, false><<<grid, kTpb, bytes, s>>>(a);
-        else band_scan_kernel<false, false><<<grid, kTpb, bytes, s>>>(a);
+    const bool cands = a.min_size < kCandThreshold;
+    const int v = (a.mad_add ? 1 : 0) | (a.indep ? 2 : 0) | (cands ? 4 : 0);
+    switch (v) {
+        case 0: band_scan_kernel<false, false, false><<<grid, kTpb, bytes, s>>>(a); break;
+        case 1: band_scan_kernel<true, false, false><<<grid, kTpb, bytes, s>>>(a); break;
+        case 2: band_scan_kernel<false, true, false><<<grid, kTpb, bytes, s>>>(a); break;
+        case 3: band_scan_kernel<true, true, false><<<grid, kTpb, bytes, s>>>(a); break;
+        case 4: band_scan_kernel<false, false, true><<<grid, kTpb, bytes, s>>>(a); break;
+        case 5: band_scan_kernel<true, false, true><<<grid, kTpb, bytes, s>>>(a); break;
+        case 6: band_scan_kernel<false, true, true><<<grid, kTpb, bytes, s>>>(a); break;
+        default: band_scan_kernel<true, true, true><<<grid, kTpb, bytes, s>>>(a); break;
     }
     return cudaGetLastError();
 }
