@@ -327,14 +327,12 @@ void Server::run() {
             }
             live = active;
         }
-        bool ok;
         {
             std::lock_guard<std::mutex> glock(ctx().mu);
-            ok = step(live);
-        }
-        if (!ok) {  // a CUDA failure: fail what was in flight
-            for (Job* j : live)
-                if (j->state == kRunning) complete(j, -1, false);
+            if (!step(live)) {  // a CUDA failure: fail what was in flight
+                for (Job* j : live)
+                    if (j->state == kRunning) complete(j, -1, false);
+            }
         }
     }
     // Shutting down: release device memory of unfinished jobs.

@@ -1,0 +1,33 @@
+"""CPU checks of the autotuner's rule derivation (slime_b200/autotune.py) on synthetic timings."""
+from slime_b200.autotune import PERIOD, derive
+
+
+def grid(indep_from, band_rule):
+    rows = []
+    for r in (30_000, 100_000, 300_000, 600_000, 1_000_000):
+        w = 2 * r + 1
+        for thr in range(40, 62, 2):
+            p = {"radius": r, "threshold": thr, "centres": w * w, "general_s": 1.0,
+                 "indep_s": 0.5 if thr >= indep_from else 2.0}
+            if w >= 2 * PERIOD:
+                p["band_s"] = 0.2 if band_rule(w // PERIOD, thr) else 0.9
+            rows.append(p)
+    return rows
+
+
+def test_derive_recovers_the_crossovers():
+    # Shared LCG wins from 48 on 9+ periods and from 54 on 4+ periods.
+    rows = grid(44, lambda periods, thr: (periods >= 9 and thr >= 48) or (periods >= 4 and thr >= 54))
+    band_thr, band_periods, fast_thr, fast_periods, indep_thr, indep_centres = derive(rows)
+    assert indep_thr == 44 and indep_centres == (2 * 30_000 + 1) ** 2
+    branches = {(band_thr, band_periods), (fast_thr, fast_periods)}
+    assert branches == {(48, 9), (54, 4)}
+
+
+def test_derive_never_picks_an_engine_that_loses_above_its_threshold():
+    # Independent bands win at 46 and above except at 50: the rule must start above 50.
+    rows = grid(46, lambda periods, thr: False)
+    for p in rows:
+        if p["threshold"] == 50:
+            p["indep_s"] = 1.5
+    assert derive(rows)[4] == 52
