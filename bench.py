@@ -30,7 +30,7 @@ from pathlib import Path
 ROOT = Path(__file__).resolve().parent
 sys.path.insert(0, str(ROOT))
 
-from slime_b200 import workloads  # noqa: E402
+from slime_b200 import replicas, workloads  # noqa: E402
 
 ALGO_OPS_PER_CENTRE = 4  # first-draw test per centre: add, xor, multiply-add, compare
 # dram__bytes_read.sum + dram__bytes_write.sum of one band_scan_kernel launch of this workload,
@@ -159,11 +159,18 @@ def run_reference(args, rank, world):
     print(json.dumps(line), flush=True)
 
 
-def run_other(args):
-    """One JSON line for the plain, batch or served workload (one GPU, host API timing)."""
+def run_other(args, rank=0, world=1, local_rank=0):
+    """One JSON line for the plain, batch or served workload (host API timing). The batch shards
+    its requests over the ranks (balanced by centres; the timing is the slowest rank's); plain
+    and served run on rank 0 only."""
     import numpy as np
     import torch
-    torch.cuda.set_device(0)
+    torch.cuda.set_device(local_rank)
+    dist = None
+    if args.workload == "batch" and world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=600))
     from slime_b200 import build
     from slime_b200.lib import SlimeCoreB200, SlimeServer
     build.build()
@@ -182,8 +189,9 @@ def run_other(args):
                 return [core.search(q.seed, q.radius, q.min_size, q.max_size, q.rd_min, q.center_x,
                                     q.center_z, q.max_results, 0)]
         else:
-            work = workloads.batch_searches()
-            centres = sum(q.centres for q in work)
+            everything = workloads.batch_searches()
+            work = [everything[i] for i in replicas.shard_requests(everything, rank, world)]
+            centres = sum(q.centres for q in everything)
 
             def run_ours():
                 core.lib.reset_cancel()
@@ -213,9 +221,15 @@ def run_other(args):
         t_loop = (time.perf_counter() - t0) / args.steps
         sampler.stop()
         assert all(a[0] == b[0] and np.array_equal(a[1], b[1]) for a, b in zip(res, ref))
+        if dist:
+            (t_ours, t_loop), _ = replicas.reduce_max_sum(dist, [t_ours, t_loop], [0.0], device="cuda")
+            dist.destroy_process_group()
+            if rank != 0:
+                return
         name = ("T centres/s plain 4,001^2 threshold-40 search" if args.workload == "plain"
                 else "T centres/s 64-seed mixed batch")
         line.update({
+            "n_gpus": world, "scaling": "strong" if world > 1 else "weak",
             "metric": name, "value": centres / t_ours / 1e12, "unit": "T centres/s",
             "ms_per_step": t_ours * 1e3,
             "e2e": {"value": centres / t_ours / 1e12, "unit": "T centres/s", "h2d_bytes_per_step": 48 * len(work),
@@ -308,8 +322,8 @@ def main():
         run_reference(args, rank, world)
         return
     if args.workload != "full_world":
-        if rank == 0:
-            run_other(args)
+        if args.workload == "batch" or rank == 0:
+            run_other(args, rank, world, local_rank)
         return
 
     import numpy as np
@@ -326,8 +340,7 @@ def main():
     build.build()
     core = SlimeCoreB200()
     spec = workloads.full_world_scan()
-    seed = spec.seed + rank * 0x9E3779B97F4A7C15 % (1 << 63)
-    seed = ((seed + (1 << 63)) % (1 << 64)) - (1 << 63)
+    seed = replicas.replica_seed(spec.seed, rank)
     radius = min(args.radius, workloads.WORLD_RADIUS)
     centres = (2 * radius + 1) ** 2
     out = np.zeros(spec.max_results, dtype=RESULT_DTYPE)
@@ -369,9 +382,7 @@ def main():
     sampler.stop()
     if dist:
         dist.barrier()
-        t = torch.tensor([kernel_ms, e2e_ms], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        kernel_ms, e2e_ms = t.tolist()
+        (kernel_ms, e2e_ms), _ = replicas.reduce_max_sum(dist, [kernel_ms, e2e_ms], [0.0], device="cuda")
     if rank != 0:
         if dist:
             dist.destroy_process_group()
