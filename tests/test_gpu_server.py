@@ -96,3 +96,17 @@ def test_server_small_requests_finish_while_a_large_one_runs(core):
     for q, (total, res, _) in zip(small, res_small):
         t_s, r_s = single(core, q)
         assert total == t_s and np.array_equal(res, r_s)
+
+
+def test_server_destroy_with_requests_in_flight(core):
+    """Closing the server while a large request runs and others wait ends the worker cleanly; the
+    library then serves ordinary searches as before."""
+    from slime_b200.lib import SlimeServer
+    server = SlimeServer(core=core)
+    big = Search(seed=50, center_x=0, center_z=0, radius=1_000_000, min_size=55, max_results=10)
+    tickets = [server.submit(big)] + [server.submit(q) for q in MIX[:3]]
+    assert all(server.poll(t) in (server.QUEUED, server.RUNNING, server.DONE) for t in tickets)
+    server.close()
+    q = MIX[1]
+    t_s, r_s = single(core, q)
+    assert t_s >= 0 and len(r_s) == min(t_s, q.max_results)
