@@ -43,13 +43,26 @@ def needs_build() -> bool:
 def build(force: bool = False, verbose: bool = False) -> Path:
     if not force and not needs_build():
         return LIB
+    # One object per source, compiled in parallel, then one link.
+    objdir = PKG / "_build"
+    objdir.mkdir(exist_ok=True)
+    jobs = []
+    for src in sources():
+        obj = objdir / (src.stem + ".o")
+        cmd = [nvcc(), *ARCH, *FLAGS, "-c", str(src), "-o", str(obj)]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        jobs.append((obj, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)))
+    objs = []
+    for obj, p in jobs:
+        _, err = p.communicate()
+        if p.returncode != 0:
+            raise RuntimeError(f"nvcc failed ({p.returncode}) on {obj.stem}.cu:\n{err[-6000:]}")
+        objs.append(str(obj))
     tmp = LIB.with_suffix(".so.tmp")
-    cmd = [nvcc(), *ARCH, *FLAGS, "-shared", "-o", str(tmp), *map(str, sources())]
-    if verbose:
-        print(" ".join(cmd), file=sys.stderr)
-    res = subprocess.run(cmd, capture_output=True, text=True)
+    res = subprocess.run([nvcc(), *ARCH, "-shared", "-o", str(tmp), *objs], capture_output=True, text=True)
     if res.returncode != 0:
-        raise RuntimeError(f"nvcc failed ({res.returncode}):\n{res.stderr[-6000:]}")
+        raise RuntimeError(f"nvcc link failed ({res.returncode}):\n{res.stderr[-6000:]}")
     os.replace(tmp, LIB)
     return LIB
 
