@@ -16,25 +16,24 @@
 
 namespace slime {
 
-namespace {
-
 // P(count >= k) for a 221-cell window of independent p = 0.1 cells: the expected share of
-// centres a threshold keeps, used to size each search's slice of the hit pool.
+// centres a threshold keeps, used to size a search's hit slice (batches and the server).
 double tail_share(int k) {
-    static std::vector<double> tail;
-    if (tail.empty()) {
-        std::vector<double> pmf(222, 0.0);
+    static const std::vector<double> tail = [] {  // built once (thread-safe static init)
+        std::vector<double> pmf(222, 0.0), t(223, 0.0);
         pmf[0] = std::pow(0.9, 221);
         for (int i = 1; i <= 221; ++i) pmf[i] = pmf[i - 1] * (221 - i + 1) / i * (0.1 / 0.9);
-        tail.assign(223, 0.0);
-        for (int i = 221; i >= 0; --i) tail[i] = tail[i + 1] + pmf[i];
-    }
+        for (int i = 221; i >= 0; --i) t[i] = t[i + 1] + pmf[i];
+        return t;
+    }();
     return tail[std::max(0, std::min(222, k))];
 }
 
 // Chunks of an area whose first draw is rejected and redrawn into a slime chunk: 104,848 of the
 // 2^48 LCG states.
 double rare_share() { return 104848.0 / 281474976710656.0; }
+
+namespace {
 
 struct Planned {
     int32_t idx;          // request index

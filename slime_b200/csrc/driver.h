@@ -171,4 +171,9 @@ struct Context {
 
 Context& ctx();
 
+// Sizing of per-search slices (batch.cu): the share of centres a threshold keeps in a window of
+// independent p = 0.1 cells, and the share of chunks that are rare redraw chunks.
+double tail_share(int min_size);
+double rare_share();
+
 }  // namespace slime

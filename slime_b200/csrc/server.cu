@@ -31,18 +31,6 @@ using Clock = std::chrono::steady_clock;
 
 enum : int32_t { kQueued = 0, kRunning = 1, kDone = 2, kFailed = -1, kUnknown = -2 };
 
-double tail_share_k(int k) {
-    static std::vector<double> tail;
-    if (tail.empty()) {
-        std::vector<double> pmf(222, 0.0);
-        pmf[0] = std::pow(0.9, 221);
-        for (int i = 1; i <= 221; ++i) pmf[i] = pmf[i - 1] * (221 - i + 1) / i * (0.1 / 0.9);
-        tail.assign(223, 0.0);
-        for (int i = 221; i >= 0; --i) tail[i] = tail[i + 1] + pmf[i];
-    }
-    return tail[std::max(0, std::min(222, k))];
-}
-
 struct Job {
     int64_t ticket = 0;
     SearchSpec q{};
@@ -103,7 +91,7 @@ void plan_job(Job& j, const Context& c) {
     const int64_t W = 2 * q.rd_max + 1;
     const int32_t algo = c.engine_for(q);
     const double centres = (double)W * (double)W;
-    const double expect = centres * tail_share_k(q.min_size);
+    const double expect = centres * tail_share(q.min_size);
     j.band = q.min_size >= 28 && algo != kAlgoGeneral && expect * 1.5 < (double)(16u << 20);
     if (!j.band) {
         // The single search's term tables and hit buffer (library buffers, counted for gating).
@@ -115,7 +103,7 @@ void plan_job(Job& j, const Context& c) {
     j.area_z0 = (int32_t)((int64_t)q.center_z - q.rd_max);
     j.hit_cap = (uint64_t)std::min<double>((double)(16u << 20), 2.0 * expect + 65536.0);
     const double halo = (double)(W + 16) * (double)(W + 16);
-    j.rare_cap = (uint32_t)std::min<double>(1 << 20, 3.0 * halo * (104848.0 / 281474976710656.0) + 1024.0);
+    j.rare_cap = (uint32_t)std::min<double>(1 << 20, 3.0 * halo * rare_share() + 1024.0);
     j.bytes = align256((size_t)(j.g.width_u + 16) * 8) +
               align256((size_t)j.g.ngroups * j.g.vrows_alloc * band_row_words(j.g.indep) * 4) +
               align256((size_t)j.hit_cap * sizeof(Hit)) + align256((size_t)j.rare_cap * sizeof(int2)) + 256;
