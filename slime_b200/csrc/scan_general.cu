@@ -5,7 +5,9 @@
 // is kept. Design on B200: a persistent grid walks (x tile, z band) tiles; each warp evaluates
 // 32 x-adjacent chunks per ballot and publishes the words of a row into a 32-row shared ring;
 // each thread keeps rolling 17x17 square counts for its centre columns (square >= circle and
-// square - 68 <= circle), and only square survivors get the exact circle count. Kept centres are
+// square - 68 <= circle), and only square survivors get the exact circle count. Survivors are
+// queued per warp and counted lane-parallel (one centre per lane) while their 17 rows are still in
+// the ring, so a warp never runs the 17-row count with most lanes idle. Kept centres are
 // histogrammed by count and those at or above `emit_min` are appended with one atomic per warp.
 #include "engine.h"
 
@@ -27,11 +29,54 @@ __device__ __forceinline__ uint32_t slice17(const uint32_t* row, int word, int l
     return __funnelshift_r(row[word], row[word + 1], lane) & 0x1FFFFu;
 }
 
+constexpr int kCandCap = 64;   // per warp: square survivors waiting for their exact count
+constexpr int kCandAge = 14;   // rows a survivor may wait: its rows stay in the 32-row ring
+
+// Exact counts of the warp's queued centres (entry = column << 16 | centre row in the tile), one
+// per lane, 32 at a time; counts in range are histogrammed, those >= emit_min emitted. The rows
+// read are at most kCandAge + 16 behind the newest, so the next row written never overwrites them.
+template <int TPB, int CPT>
+__device__ __forceinline__ void general_flush(const ScanArgs& a, const uint32_t* ring, unsigned int* hist_s,
+                                              const uint32_t* cand, int ncand, int x_base, int z_base, int lane) {
+    using T = GeneralTile<TPB, CPT>;
+    __syncwarp();
+    for (int base = 0; base < ncand; base += 32) {
+        bool want = false;
+        int exact = 0, col = 0, j = 0;
+        if (base + lane < ncand) {
+            const uint32_t e = cand[base + lane];
+            col = (int)(e >> 16);
+            j = (int)(e & 0xFFFFu);
+            const int word = col >> 5, bit = col & 31;
+#pragma unroll
+            for (int i = 0; i < 17; ++i)
+                exact += __popc(slice17(ring + ((j + i) & 31) * T::kStride, word, bit) & window_row_mask(i));
+            if (exact >= a.min_size && exact <= a.max_size) {
+                atomicAdd(&hist_s[exact], 1u);
+                want = exact >= a.emit_min;
+            }
+        }
+        const unsigned m = __ballot_sync(kFull, want);
+        if (m) {
+            const int leader = __ffs(m) - 1;
+            unsigned long long pos = 0;
+            if (lane == leader) pos = atomicAdd(a.emitted, (unsigned long long)__popc(m));
+            pos = __shfl_sync(kFull, pos, leader);
+            if (want) {
+                const unsigned long long idx = pos + __popc(m & ((1u << lane) - 1u));
+                if (idx < a.cap) a.out[idx] = Hit{exact, a.area_x0 + x_base + col, a.area_z0 + z_base + j};
+            }
+        }
+    }
+    __syncwarp();
+}
+
 template <int TPB, int CPT>
 __global__ void __launch_bounds__(TPB) general_scan_kernel(const ScanArgs a) {
     using T = GeneralTile<TPB, CPT>;
     __shared__ __align__(16) uint32_t ring[32 * T::kStride];
     __shared__ unsigned int hist_s[kHistBins];
+    __shared__ uint32_t cand_s[T::kWarps][kCandCap];
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     for (int i = tid; i < kHistBins; i += TPB) hist_s[i] = 0;
@@ -58,6 +103,8 @@ __global__ void __launch_bounds__(TPB) general_scan_kernel(const ScanArgs a) {
             sq[k] = 0;
         }
 
+        uint32_t* cand = cand_s[warp];
+        int ncand = 0, first_r = 0;  // warp-uniform: queued survivors, row of the oldest
         for (int r = 0; r < in_h; ++r) {
             const uint64_t zt = a.zt[z_base + r];
             uint32_t words[CPT];
@@ -79,6 +126,10 @@ __global__ void __launch_bounds__(TPB) general_scan_kernel(const ScanArgs a) {
             }
             __syncthreads();
 
+            if (ncand && r - first_r >= kCandAge) {
+                general_flush<TPB, CPT>(a, ring, hist_s, cand, ncand, x_base, z_base, lane);
+                ncand = 0;
+            }
 #pragma unroll
             for (int k = 0; k < CPT; ++k) {
                 const int word = warp * CPT + k;
@@ -88,42 +139,25 @@ __global__ void __launch_bounds__(TPB) general_scan_kernel(const ScanArgs a) {
                     sq[k] += __popc(slice17(row, word, lane));
                     if (r >= 17) sq[k] -= __popc(slice17(ring + ((r - 17) & 31) * T::kStride, word, lane));
                 }
-                bool want = false;
-                int exact = 0;
-                int cz = 0;
-                if (active && r >= 16 && sq[k] >= a.min_size && (no_upper || sq[k] <= a.max_size + 68)) {
-                    const int j = r - 16;  // centre row within the tile
-                    const int cx = a.area_x0 + x_base + col;
-                    cz = a.area_z0 + z_base + j;
-                    bool inside = true;
-                    if (a.rd_min_sq != 0) {
-                        const int64_t dx = (int64_t)cx - a.center_x, dz = (int64_t)cz - a.center_z;
-                        inside = dx * dx + dz * dz >= a.rd_min_sq;
-                    }
-                    if (inside) {
-#pragma unroll
-                        for (int i = 0; i < 17; ++i)
-                            exact += __popc(slice17(ring + ((j + i) & 31) * T::kStride, word, lane) &
-                                            window_row_mask(i));
-                        if (exact >= a.min_size && exact <= a.max_size) {
-                            atomicAdd(&hist_s[exact], 1u);
-                            want = exact >= a.emit_min;
-                        }
-                    }
+                bool flag = active && r >= 16 && sq[k] >= a.min_size && (no_upper || sq[k] <= a.max_size + 68);
+                if (flag && a.rd_min_sq != 0) {
+                    const int64_t dx = (int64_t)(a.area_x0 + x_base + col) - a.center_x;
+                    const int64_t dz = (int64_t)(a.area_z0 + z_base + r - 16) - a.center_z;
+                    flag = dx * dx + dz * dz >= a.rd_min_sq;
                 }
-                const unsigned m = __ballot_sync(kFull, want);
+                const unsigned m = __ballot_sync(kFull, flag);
                 if (m) {
-                    const int leader = __ffs(m) - 1;
-                    unsigned long long base = 0;
-                    if (lane == leader) base = atomicAdd(a.emitted, (unsigned long long)__popc(m));
-                    base = __shfl_sync(kFull, base, leader);
-                    if (want) {
-                        const unsigned long long idx = base + __popc(m & ((1u << lane) - 1u));
-                        if (idx < a.cap) a.out[idx] = Hit{exact, a.area_x0 + x_base + col, cz};
+                    if (ncand + __popc(m) > kCandCap) {
+                        general_flush<TPB, CPT>(a, ring, hist_s, cand, ncand, x_base, z_base, lane);
+                        ncand = 0;
                     }
+                    if (ncand == 0) first_r = r;
+                    if (flag) cand[ncand + __popc(m & ((1u << lane) - 1u))] = ((uint32_t)col << 16) | (uint32_t)(r - 16);
+                    ncand += __popc(m);
                 }
             }
         }
+        if (ncand) general_flush<TPB, CPT>(a, ring, hist_s, cand, ncand, x_base, z_base, lane);
         __syncthreads();  // the next tile reuses ring slots still read above
     }
     for (int i = tid; i < kHistBins; i += TPB)
