@@ -49,8 +49,8 @@ def measure(core, quick=False):
     for r in radii:
         w = 2 * r + 1
         for thr in range(40, 62, 4 if quick else 2):
-            if r >= 300_000 and thr < 44:
-                continue  # hours of band work for no decision: the general scan wins there
+            if r >= 300_000 and thr < 42:
+                continue  # minutes of band work for no decision: the general scan wins there
             point = {"radius": r, "threshold": thr, "centres": w * w}
             ref = None
             engines = [("indep", 3)] + ([("band", 2)] if w >= 2 * PERIOD else [])

@@ -114,11 +114,11 @@ struct Context {
     // from band_fast_threshold; independent bands for areas of indep_min_centres centres or more
     // from indep_min_threshold; the general scan otherwise. Defaults: the rule slime_b200/
     // autotune.py derived on B200 (slime_b200/tuning_b200.json).
-    int32_t band_min_threshold = 48;
+    int32_t band_min_threshold = 46;
     int32_t band_min_periods = 9;
-    int32_t band_fast_threshold = 52;
+    int32_t band_fast_threshold = 50;
     int32_t band_fast_periods = 4;
-    int32_t indep_min_threshold = 44;
+    int32_t indep_min_threshold = 42;
     int64_t indep_min_centres = 3600120001;
     int64_t last_rare = 0;             // rare redraw chunks found by the last band search
     int64_t band_fallbacks = 0;        // band searches redone by the general scan

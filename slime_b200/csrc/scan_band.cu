@@ -145,6 +145,16 @@ __host__ __device__ constexpr uint32_t group_union_mask(int r) {
     return ((1u << (2 * h + 4)) - 1u) << (8 - h);
 }
 
+// Row `r` (0..19) of the union of the 4 windows of the 2x2 sub-group (sx, sy) of a 4x4 group
+// (centres dx = 2sx, 2sx+1 and dz = 2sy, 2sy+1), as a 20-bit column mask; 0 outside its rows.
+__host__ __device__ constexpr uint32_t subgroup_union_mask(int r, int sx, int sy) {
+    int h = -1;
+    for (int dz = 2 * sy; dz < 2 * sy + 2; ++dz)
+        if (r - dz >= 0 && r - dz <= 16 && window_half_width(r - dz) > h) h = window_half_width(r - dz);
+    return h < 0 ? 0u : ((1u << (2 * h + 2)) - 1u) << (2 * sx + 8 - h);
+}
+constexpr int kSubgroupThreshold = 52;  // at or below: also test the four 2x2 sub-group unions
+
 // Exact window counts of the 16 centres of group g of word `word` for one combo, from the 20
 // ring rows of strips st-4..st. Lanes 0..19 fetch one 20-column row slice each. First the whole
 // union of the 16 windows (332 cells; `umask` = this lane's row of it) is counted with one
@@ -240,14 +250,30 @@ __device__ __forceinline__ void flush_cands(BandSmem& S, const BandArgs& a, cons
                 cmh &= word + 1 < kWords ? column_mask(a, T, word + 1, combo_phase<kIndep>(combo)) : 0u;
             }
             const int wh = min(word + 1, kWords - 1);
-            int sum = 0;
+            if (a.min_size > kSubgroupThreshold) {
+                int sum = 0;
 #pragma unroll
-            for (int r = 0; r < 20; ++r) {
-                const uint32_t lo = combo_word<kIndep>(S, r0 + r, combo, fx, word) & cml;
-                const uint32_t hi = combo_word<kIndep>(S, r0 + r, combo, fx, wh) & cmh;
-                sum += __popc(__funnelshift_r(lo, hi, 4 * g) & group_union_mask(r));
+                for (int r = 0; r < 20; ++r) {
+                    const uint32_t lo = combo_word<kIndep>(S, r0 + r, combo, fx, word) & cml;
+                    const uint32_t hi = combo_word<kIndep>(S, r0 + r, combo, fx, wh) & cmh;
+                    sum += __popc(__funnelshift_r(lo, hi, 4 * g) & group_union_mask(r));
+                }
+                pass = sum >= a.min_size;
+            } else {
+                int sum = 0, s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+#pragma unroll
+                for (int r = 0; r < 20; ++r) {
+                    const uint32_t lo = combo_word<kIndep>(S, r0 + r, combo, fx, word) & cml;
+                    const uint32_t hi = combo_word<kIndep>(S, r0 + r, combo, fx, wh) & cmh;
+                    const uint32_t x = __funnelshift_r(lo, hi, 4 * g);
+                    sum += __popc(x & group_union_mask(r));
+                    s0 += __popc(x & subgroup_union_mask(r, 0, 0));
+                    s1 += __popc(x & subgroup_union_mask(r, 1, 0));
+                    s2 += __popc(x & subgroup_union_mask(r, 0, 1));
+                    s3 += __popc(x & subgroup_union_mask(r, 1, 1));
+                }
+                pass = sum >= a.min_size && max(max(s0, s1), max(s2, s3)) >= a.min_size;
             }
-            pass = sum >= a.min_size;
         }
         for (unsigned pm = __ballot_sync(kFull, pass); pm; pm &= pm - 1) {
             const uint32_t ee = __shfl_sync(kFull, e, __ffs(pm) - 1);
@@ -299,23 +325,22 @@ __device__ __forceinline__ void second_test(BandSmem& S, const BandArgs& a, cons
     }
     const int total = __shfl_sync(kFull, pos, 31);
     if (total == 0) return;
-    if (total > kCandCap) {  // a dense word set (low threshold): count this combo's groups now
-        for (unsigned todo = __ballot_sync(kFull, gm != 0); todo; todo &= todo - 1) {
-            const int word = __ffs(todo) - 1;
-            for (uint32_t gw = __shfl_sync(kFull, gm, word); gw; gw &= gw - 1)
-                exact_group<kMasked, kIndep>(S, a, T, combo, fx, word, __ffs(gw) - 1, st, lane, umask);
-        }
-        return;
-    }
-    if (ncand + total > kCandCap) {
+    // Survivor i of this combo (lane order) goes to list slot ncand + i - placed; a full list is
+    // counted (one call site) and refilled until every survivor is placed.
+    for (int placed = 0;;) {
+        const int room = kCandCap - ncand;
+        int idx = pos - n;
+        for (uint32_t gw = gm; gw; gw &= gw - 1, ++idx)
+            if (idx >= placed && idx < placed + room)
+                S.cand[warp][ncand + idx - placed] = ((uint32_t)combo << 24) | ((uint32_t)lane << 19) |
+                                                     ((uint32_t)(__ffs(gw) - 1) << 16) | (uint32_t)st;
+        const int took = min(room, total - placed);
+        ncand += took;
+        placed += took;
+        if (placed == total) break;
         flush_cands<kMasked, kIndep>(S, a, T, fx, warp, lane, umask, ncand);
         ncand = 0;
     }
-    int idx = ncand + pos - n;
-    for (uint32_t gw = gm; gw; gw &= gw - 1)
-        S.cand[warp][idx++] = ((uint32_t)combo << 24) | ((uint32_t)lane << 19) | ((uint32_t)(__ffs(gw) - 1) << 16) |
-                              (uint32_t)st;
-    ncand += total;
     __syncwarp();
 }
 
