@@ -163,12 +163,17 @@ int32_t slime_b200_microbench(int32_t kind, int32_t iters, double* lane_ops_per_
  * return value and ranked output as search_slime_clusters_gpu_v1_centered, without precise
  * scoring. Its working memory is one fixed 4 MiB array inside the library, which every GPU that
  * loads the library holds until the process exits; the call makes no cudaMalloc, cudaFree,
- * cudaMallocHost or host heap allocation. Limits: rd_max <= 8191 and max_results <= 65536;
- * larger requests return -1 with an error text (slime_b200_last_error). The first call on a
- * device looks up the array's device address (set-up), so make that first call before any
- * stream capture. All calls share the array: calls that overlap on the GPU (for example from
- * several processes or contexts on one device at once) race; calls from one process are
- * serialised. Runs on the legacy default stream. */
+ * cudaMallocHost or host heap allocation (error texts go to a fixed buffer). Limits: rd_max <= 8191
+ * and max_results <= 65536; larger requests return -1 with an error text (slime_b200_last_error).
+ * A call can also return -1 if a single 64-row band of the area holds more than about 327k centres
+ * at or above the count gate its max_results implies (possible only with max_results near 65536
+ * and a wide area). The first call on a device looks up the array's device address (set-up) and
+ * caches it per device ordinal, so make that first call before any stream capture; a device
+ * reset invalidates the cached address, so call cleanup_gpu_resources() after resetting a device.
+ * The array exists once per process and device (per loaded module and context), and every call
+ * in the process shares it: the library lock serialises calls from the threads of one process,
+ * and calls that could still overlap on the GPU (another context of the same process on the same
+ * device) race. Runs on the legacy default stream. */
 int64_t slime_b200_search_noalloc(int64_t seed, int64_t rd_max, int32_t min_size, int32_t max_size,
                                   int64_t rd_min, int32_t search_center_x, int32_t search_center_z,
                                   ExtChunkResult* results_buffer, int32_t max_results);

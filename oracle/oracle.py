@@ -23,7 +23,12 @@ HERE = Path(__file__).resolve().parent
 ORACLE_SO = HERE / "_build" / "libslime_oracle.so"
 REF_SO = HERE / "_ref" / "libslimecore_ref.so"
 REF_GPU_SO = HERE / "_ref" / "libslimecore_gpu_ref.so"
-REF_SRC_DIR = Path(os.environ.get("SLIME_REFERENCE_DIR", "/root/reference"))
+
+
+def reference_dir(ref_dir=None):
+    """The reference source tree: the argument, else $SLIME_REFERENCE_DIR, else None (no default)."""
+    d = ref_dir if ref_dir is not None else os.environ.get("SLIME_REFERENCE_DIR")
+    return Path(d) if d else None
 
 
 class ExtChunkResult(C.Structure):
@@ -50,11 +55,13 @@ class YConfig(C.Structure):
                 ("y_max", C.c_int32), ("y_step", C.c_int32)]
 
 
-def build(ref: bool = True) -> None:
-    """Build the restatement, and the reference CPU library when its source is present."""
+def build(ref: bool = True, ref_dir=None) -> None:
+    """Build the restatement, and the reference libraries when the reference source tree is given
+    (``ref_dir`` or ``$SLIME_REFERENCE_DIR``) and present."""
     subprocess.run(["make", "-C", str(HERE), "oracle"], check=True, capture_output=True)
-    if ref and (REF_SRC_DIR / "SlimeCore.cpp").exists():
-        subprocess.run(["make", "-C", str(HERE), "ref", "ref_gpu", f"REF_DIR={REF_SRC_DIR}"],
+    src = reference_dir(ref_dir)
+    if ref and src is not None and (src / "SlimeCore.cpp").exists():
+        subprocess.run(["make", "-C", str(HERE), "ref", "ref_gpu", f"REF_DIR={src}"],
                        check=True, capture_output=True)
 
 

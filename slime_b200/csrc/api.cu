@@ -26,10 +26,12 @@ Context& ctx() {
 }
 
 void Context::set_error(const char* where, cudaError_t e) {
-    char buf[256];
-    std::snprintf(buf, sizeof(buf), "%s: %s", where, cudaGetErrorString(e));
-    last_error = buf;
+    std::snprintf(last_error, sizeof(last_error), "%s: %s", where, cudaGetErrorString(e));
     cudaGetLastError();  // clear a sticky launch error so later calls start clean
+}
+
+void Context::set_error_text(const char* text) {
+    std::snprintf(last_error, sizeof(last_error), "%s", text);
 }
 
 bool Context::ensure_device() {
@@ -529,6 +531,7 @@ void set_gpu_v34_rng_override(int32_t value) { set_gpu_v1_rng_override(value); }
 void cleanup_gpu_resources(void) {
     std::lock_guard<std::mutex> lock(ctx().mu);
     ctx().release();
+    slime::forget_noalloc_scratch();
 }
 
 bool is_slime_chunk_c(int64_t seed, int64_t cx, int64_t cz) { return slime::is_slime(seed, cx, cz); }
@@ -553,7 +556,7 @@ void slime_b200_set_engine(int32_t mode, int32_t band_min_threshold) {
     if (band_min_threshold >= 28 && band_min_threshold <= 221) ctx().band_min_threshold = band_min_threshold;
 }
 
-const char* slime_b200_last_error(void) { return ctx().last_error.c_str(); }
+const char* slime_b200_last_error(void) { return ctx().last_error; }
 
 int32_t slime_b200_set_engine_rule(const int64_t* rule, int32_t n) {
     if (!rule || n != 6) return -1;

@@ -105,7 +105,7 @@ bool Context::collect_band(const SearchSpec& q, int32_t area_x0, int32_t area_z0
 
 int32_t Context::search_batch(const SearchSpec* reqs, int32_t n, ExtChunkResult* results, int64_t* totals) {
     if (n < 0 || (n > 0 && (!reqs || !results || !totals))) {
-        last_error = "batch: invalid arguments";
+        set_error_text("batch: invalid arguments");
         return -1;
     }
     if (!ensure_device() || !ensure_band()) return -1;

@@ -82,7 +82,8 @@ struct Context {
     int sm_count = 148;
     cudaStream_t stream = nullptr;
     void* pinned = nullptr;
-    std::string last_error;
+    // Last error text: a fixed buffer, so that recording an error never allocates.
+    char last_error[256] = {};
 
     DeviceBuffer<uint64_t> xt, zt;
     DeviceBuffer<Hit> hits;
@@ -144,6 +145,7 @@ struct Context {
     cudaEvent_t ev_a = nullptr, ev_b = nullptr;
 
     void set_error(const char* where, cudaError_t e);
+    void set_error_text(const char* text);
     bool ensure_device();
     bool ensure_y_tables();
     void release();
@@ -170,6 +172,9 @@ struct Context {
 };
 
 Context& ctx();
+
+// Forgets the cached device addresses of the no-alloc search's scratch array (noalloc.cu).
+void forget_noalloc_scratch();
 
 // Sizing of per-search slices (batch.cu): the share of centres a threshold keeps in a window of
 // independent p = 0.1 cells, and the share of chunks that are rare redraw chunks.

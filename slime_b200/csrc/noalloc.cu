@@ -9,12 +9,16 @@
 // process exits), and it calls no cudaMalloc, cudaFree, cudaMallocHost or host heap allocation.
 //
 // Limits: search radius <= kMaxRadius chunks, max_results <= kMaxResults. Larger requests are
-// rejected with -1 and an error text (slime_b200_last_error). No precise AFK scoring.
+// rejected with -1 and an error text (slime_b200_last_error). No precise AFK scoring. A call also
+// fails with -1 in the unlikely case that a single 64-row band emits more than kHitCap centres at
+// or above its gate (the gate is the exact count the histogram pass chose for max_results).
+//
+// Calls hold the library lock for their whole duration, like every other entry point, so error
+// texts (a fixed buffer of the library) are written without racing another thread's search.
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
 #include <cstring>
-#include <mutex>
 
 #include "../../include/slimecore_b200.h"
 #include "driver.h"
@@ -36,7 +40,9 @@ constexpr int kCopyChunk = 2048;                             // hits copied back
 // symbol, never a device address: the kernels get the address from cudaGetSymbolAddress.
 static __device__ __align__(256) unsigned char g_scratch[kScratchBytes];
 
-std::mutex g_mu;
+// Device address of g_scratch per device ordinal, looked up once (under the library lock).
+// cleanup_gpu_resources() forgets them; a device reset by the caller unloads the module, so a
+// caller that resets a device must call cleanup_gpu_resources() before the next search here.
 unsigned char* g_scratch_ptr[kMaxDevices] = {};
 
 // Set-up, once per device, with that device current: the device address of g_scratch.
@@ -48,8 +54,6 @@ bool scratch_for_current_device(unsigned char** out) {
         return false;
     }
     if (!g_scratch_ptr[dev]) {
-        // Room for error texts, so that later failures record them without allocating.
-        ctx().last_error.reserve(256);
         void* p = nullptr;
         e = cudaGetSymbolAddress(&p, g_scratch);
         if (e != cudaSuccess || !p) {
@@ -72,16 +76,20 @@ bool ranks_before(const ExtChunkResult& a, const ExtChunkResult& b) {
 
 }  // namespace
 
+void forget_noalloc_scratch() {
+    for (auto& p : g_scratch_ptr) p = nullptr;
+}
+
 int64_t search_noalloc(int64_t seed, int64_t rd_max, int32_t min_size, int32_t max_size,
                        int64_t rd_min, int32_t cx, int32_t cz, ExtChunkResult* results,
                        int32_t max_results) {
+    std::lock_guard<std::mutex> lock(ctx().mu);
     if (!validate_search(rd_max, min_size, max_size, rd_min, cx, cz, results, max_results)) return -1;
     if (rd_max > kMaxRadius || max_results > kMaxResults) {
-        ctx().last_error = "no-alloc search: radius above 8191 chunks or max_results above 65536 "
-                           "(the fixed 4 MiB scratch array does not hold larger searches)";
+        ctx().set_error_text("no-alloc search: radius above 8191 chunks or max_results above 65536 "
+                             "(the fixed 4 MiB scratch array does not hold larger searches)");
         return -1;
     }
-    std::lock_guard<std::mutex> lock(g_mu);
     unsigned char* base = nullptr;
     if (!scratch_for_current_device(&base)) return -1;
     const int64_t width = 2 * rd_max + 1, height = width;
@@ -168,7 +176,7 @@ int64_t search_noalloc(int64_t seed, int64_t rd_max, int32_t min_size, int32_t m
             if (!run(gate, tz * band_h, rows, &n, nullptr)) return -1;
             if (n <= kHitCap) break;
             if (bands == 1) {
-                ctx().last_error = "no-alloc search: one 64-row band overflows the scratch hit list";
+                ctx().set_error_text("no-alloc search: one 64-row band overflows the scratch hit list");
                 return -1;
             }
             bands = (bands + 1) / 2;

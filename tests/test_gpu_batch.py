@@ -1,11 +1,14 @@
-"""GPU parity of the batched search (slime_b200_search_batch) with the single search.
+"""GPU parity of the batched search (slime_b200_search_batch).
 
 Every request of a batch must come back exactly as the single search returns it (same total,
-same ranked records), whether it ran in the shared persistent launch or on its own."""
+same ranked records), whether it ran in the shared persistent launch or on its own, and exactly as
+the reference returns it: requests up to radius 20k against the reference CPU library, and the
+largest ones against the reference GPU library built for sm_100a (tests/refcheck.py)."""
 import numpy as np
 import pytest
 
 from slime_b200.workloads import Search
+from tests.refcheck import CPU_MAX_RADIUS, check_against_reference
 
 pytestmark = pytest.mark.gpu
 
@@ -59,7 +62,10 @@ def test_batch_mixed_requests(core):
     ]
     single = singles(core, searches)
     assert core.lib.get_gpu_v1_algorithm() == 300
-    check_same(core.search_batch(searches), single)
+    batch = core.search_batch(searches)
+    check_same(batch, single)
+    for i, (q, (total, res)) in enumerate(zip(searches, batch)):
+        check_against_reference(q, total, res, f"mixed batch request {i}")
 
 
 def test_batch_invalid_request_is_reported_and_others_run(core):
@@ -80,4 +86,12 @@ def test_batch_of_the_64_seed_workload(core):
     from slime_b200 import workloads
     searches = workloads.batch_searches()
     assert len(searches) == 64
-    check_same(core.search_batch(searches), singles(core, searches))
+    batch = core.search_batch(searches)
+    check_same(batch, singles(core, searches))
+    # Against the reference: every request the CPU library runs in well under a second, and the
+    # four largest on the reference GPU library.
+    small = [i for i, q in enumerate(searches) if q.radius <= CPU_MAX_RADIUS]
+    large = sorted(range(len(searches)), key=lambda i: -searches[i].radius)[:4]
+    assert len(small) >= 30
+    for i in small + large:
+        check_against_reference(searches[i], *batch[i], f"64-seed batch request {i}")

@@ -1,10 +1,12 @@
 """GPU tests of the search server (slime_b200_server_*): results in the mix are exactly the
-single search's results, admission respects the device-memory budget, and continuous batching
-lets small requests finish while a large one is in flight."""
+single search's results and the reference's (tests/refcheck.py: the reference CPU library up to
+radius 20k, its GPU library above), admission respects the device-memory budget, and continuous
+batching lets small requests finish while a large one is in flight."""
 import numpy as np
 import pytest
 
 from slime_b200.workloads import Search
+from tests.refcheck import check_against_reference
 
 pytestmark = pytest.mark.gpu
 
@@ -53,11 +55,24 @@ def test_server_results_in_the_mix_equal_the_single_search(core):
     from slime_b200.lib import SlimeServer
     with SlimeServer(core=core) as server:
         got = run_all(server, MIX)
-    for q, (total, res, lat) in zip(MIX, got):
+    for i, (q, (total, res, lat)) in enumerate(zip(MIX, got)):
         t_s, r_s = single(core, q)
         assert total == t_s
         assert np.array_equal(res, r_s)
         assert lat > 0
+        check_against_reference(q, total, res, f"served request {i}")
+
+
+def test_server_near_world_request_against_the_reference(core):
+    """A near-world request (radius 1.5M, 9e12 centres) served beside small ones, compared with
+    the reference GPU library."""
+    from slime_b200.lib import SlimeServer
+    near_world = Search(seed=-5_501_234_567_890, center_x=200_000, center_z=-300_000,
+                        radius=1_500_000, min_size=60, max_results=500)
+    with SlimeServer(core=core) as server:
+        got = run_all(server, [near_world] + MIX[:4])
+    for i, (q, (total, res, _)) in enumerate(zip([near_world] + MIX[:4], got)):
+        check_against_reference(q, total, res, f"near-world mix request {i}")
 
 
 def test_server_memory_budget_admission(core):
@@ -93,6 +108,7 @@ def test_server_small_requests_finish_while_a_large_one_runs(core):
     assert max(lat for _, _, lat in res_small) < lat_l
     t_s, r_s = single(core, large)
     assert total_l == t_s and np.array_equal(res_l, r_s)
+    check_against_reference(large, total_l, res_l, "large request")
     for q, (total, res, _) in zip(small, res_small):
         t_s, r_s = single(core, q)
         assert total == t_s and np.array_equal(res, r_s)
