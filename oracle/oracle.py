@@ -61,8 +61,8 @@ def build(ref: bool = True, ref_dir=None) -> None:
     subprocess.run(["make", "-C", str(HERE), "oracle"], check=True, capture_output=True)
     src = reference_dir(ref_dir)
     if ref and src is not None and (src / "SlimeCore.cpp").exists():
-        subprocess.run(["make", "-C", str(HERE), "ref", "ref_gpu", f"REF_DIR={src}"],
-                       check=True, capture_output=True)
+        subprocess.run(["make", "-C", str(HERE), "ref", "ref_gpu", "ref_biome", "ref_biome_gpu",
+                        f"REF_DIR={src}"], check=True, capture_output=True)
 
 
 def _ptr(a: np.ndarray):
@@ -235,3 +235,159 @@ def python_is_slime(seed: int, cx: int, cz: int) -> bool:
         val = bits % 10
         if bits - val + 9 <= 0x7FFFFFFF:
             return val == 0
+
+
+# ---- biome filter checkers -----------------------------------------------------------------------
+
+BIOME_ORACLE_SO = HERE / "_build" / "libbiome_oracle.so"
+REF_BIOME_HOST_SO = HERE / "_ref" / "libmcgpu_host_ref.so"
+REF_BIOME_GPU_SO = {"fmad": HERE / "_ref" / "libmcgpu_ref_fmad.so",
+                    "nofmad": HERE / "_ref" / "libmcgpu_ref_nofmad.so"}
+
+
+def _i32(a):
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+class _BiomeCalls:
+    """Shared call shapes of the biome checkers (prefix `bo_` or `refb_`)."""
+
+    def _bind(self, lib, p):
+        u64p = vp = C.c_void_p
+        i32 = C.c_int32
+        getattr(lib, p + "xoroshiro_nextlong").argtypes = [u64p, i32, i32, vp]
+        getattr(lib, p + "xperlin_sample").argtypes = [vp, vp, vp, vp, i32, vp]
+        getattr(lib, p + "climate6").argtypes = [C.c_uint64, i32, vp, vp, vp, i32, vp]
+        getattr(lib, p + "depth_spline").argtypes = [vp]
+        getattr(lib, p + "depth_spline").restype = C.c_float
+        getattr(lib, p + "biome_at").argtypes = [i32, C.c_uint64, i32, vp, vp, vp, i32, vp]
+        getattr(lib, p + "biome_at").restype = i32
+        getattr(lib, p + "filter").argtypes = [i32, C.c_uint64, i32, vp, vp, i32, i32, vp]
+        getattr(lib, p + "filter").restype = i32
+        self.lib, self.p = lib, p
+
+    def _f(self, name):
+        return getattr(self.lib, self.p + name)
+
+    def xoroshiro(self, seeds, steps):
+        s = np.ascontiguousarray(seeds, dtype=np.uint64)
+        out = np.zeros((len(s), steps), dtype=np.uint64)
+        self._f("xoroshiro_nextlong")(_ptr(s), len(s), steps, _ptr(out))
+        return out
+
+    def perlin(self, seeds, xs, ys, zs):
+        s = np.ascontiguousarray(seeds, dtype=np.uint64)
+        x, y, z = (np.ascontiguousarray(a, dtype=np.float64) for a in (xs, ys, zs))
+        out = np.zeros(len(s), dtype=np.float64)
+        self._f("xperlin_sample")(_ptr(s), _ptr(x), _ptr(y), _ptr(z), len(s), _ptr(out))
+        return out
+
+    def climate6(self, world_seed, xs, ys, zs, large=0):
+        x, y, z = _i32(xs), _i32(ys), _i32(zs)
+        out = np.zeros((len(x), 6), dtype=np.int32)
+        self._f("climate6")(world_seed & (2**64 - 1), large, _ptr(x), _ptr(y), _ptr(z), len(x), _ptr(out))
+        return out
+
+    def depth_spline(self, v4):
+        v = np.ascontiguousarray(v4, dtype=np.float32)
+        return float(self._f("depth_spline")(_ptr(v)))
+
+    def biome_at(self, version, world_seed, xs, ys, zs, large=0):
+        x, y, z = _i32(xs), _i32(ys), _i32(zs)
+        out = np.zeros(len(x), dtype=np.int32)
+        rc = self._f("biome_at")(version, world_seed & (2**64 - 1), large, _ptr(x), _ptr(y), _ptr(z),
+                                 len(x), _ptr(out))
+        assert rc == 0
+        return out
+
+    def filter(self, version, world_seed, cx, cz, flags, large=0):
+        x, z = _i32(cx), _i32(cz)
+        out = np.zeros(len(x), dtype=np.int32)
+        rc = self._f("filter")(version, world_seed & (2**64 - 1), large, _ptr(x), _ptr(z), len(x),
+                               flags, _ptr(out))
+        assert rc == 0
+        return out
+
+
+class BiomeOracle(_BiomeCalls):
+    """The plain-C restatement of the biome filter (biome_oracle.c)."""
+
+    def __init__(self, path: Path = BIOME_ORACLE_SO):
+        if not Path(path).exists():
+            build(ref=False)
+        self._bind(C.CDLL(str(path)), "bo_")
+
+
+class RefBiomeHost(_BiomeCalls):
+    """The reference biome module's own device math compiled for the CPU (ref_biome_host.cpp)."""
+
+    def __init__(self, path: Path = REF_BIOME_HOST_SO):
+        if not Path(path).exists():
+            raise FileNotFoundError(f"{path} is not built (needs the reference source tree)")
+        self._bind(C.CDLL(str(path)), "refb_")
+
+
+class RefBiomeGpu:
+    """The reference biome module (MinecraftGPUNoise.cu) built for sm_100a, with (`fmad`) or
+    without (`nofmad`) FMA contraction; its own mcgpu_* C ABI."""
+
+    def __init__(self, kind: str = "nofmad"):
+        path = REF_BIOME_GPU_SO[kind]
+        if not path.exists():
+            raise FileNotFoundError(f"{path} is not built (needs the reference source tree)")
+        lib = C.CDLL(str(path))
+        vp, i32, u64 = C.c_void_p, C.c_int32, C.c_uint64
+        lib.mcgpu_modern_ctx_create.argtypes = [i32, u64, i32]
+        lib.mcgpu_modern_ctx_create.restype = vp
+        lib.mcgpu_modern_ctx_create_ex.argtypes = [i32, u64, i32, i32]
+        lib.mcgpu_modern_ctx_create_ex.restype = vp
+        lib.mcgpu_modern_ctx_filter_candidates.argtypes = [vp, vp, vp, i32, i32, vp]
+        lib.mcgpu_modern_ctx_query.argtypes = [vp, vp, vp, vp, i32, vp]
+        lib.mcgpu_modern_ctx_destroy.argtypes = [vp]
+        lib.mcgpu_xoroshiro_nextlong_batch.argtypes = [vp, i32, i32, vp]
+        lib.mcgpu_xperlin_sample_batch.argtypes = [vp, vp, vp, vp, i32, vp]
+        lib.mcgpu_climate6_i32_fixed_seed.argtypes = [u64, vp, vp, vp, i32, vp]
+        lib.mcgpu_climate6_i32_fixed_seed_ex.argtypes = [u64, i32, vp, vp, vp, i32, vp]
+        self.lib = lib
+
+    def filter(self, version, world_seed, cx, cz, flags, large=0):
+        x, z = _i32(cx), _i32(cz)
+        h = self.lib.mcgpu_modern_ctx_create_ex(version, world_seed & (2**64 - 1), large, len(x))
+        assert h
+        try:
+            out = np.zeros(len(x), dtype=np.int32)
+            assert self.lib.mcgpu_modern_ctx_filter_candidates(h, _ptr(x), _ptr(z), len(x), flags, _ptr(out)) == 0
+            return out
+        finally:
+            self.lib.mcgpu_modern_ctx_destroy(h)
+
+    def biome_at(self, version, world_seed, xs, ys, zs, large=0):
+        x, y, z = _i32(xs), _i32(ys), _i32(zs)
+        h = self.lib.mcgpu_modern_ctx_create_ex(version, world_seed & (2**64 - 1), large, len(x))
+        assert h
+        try:
+            out = np.zeros(len(x), dtype=np.int32)
+            assert self.lib.mcgpu_modern_ctx_query(h, _ptr(x), _ptr(y), _ptr(z), len(x), _ptr(out)) == 0
+            return out
+        finally:
+            self.lib.mcgpu_modern_ctx_destroy(h)
+
+    def climate6(self, world_seed, xs, ys, zs, large=0):
+        x, y, z = _i32(xs), _i32(ys), _i32(zs)
+        out = np.zeros((len(x), 6), dtype=np.int32)
+        assert self.lib.mcgpu_climate6_i32_fixed_seed_ex(world_seed & (2**64 - 1), large, _ptr(x), _ptr(y),
+                                                         _ptr(z), len(x), _ptr(out)) == 0
+        return out
+
+    def xoroshiro(self, seeds, steps):
+        s = np.ascontiguousarray(seeds, dtype=np.uint64)
+        out = np.zeros((len(s), steps), dtype=np.uint64)
+        assert self.lib.mcgpu_xoroshiro_nextlong_batch(_ptr(s), len(s), steps, _ptr(out)) == 0
+        return out
+
+    def perlin(self, seeds, xs, ys, zs):
+        s = np.ascontiguousarray(seeds, dtype=np.uint64)
+        x, y, z = (np.ascontiguousarray(a, dtype=np.float64) for a in (xs, ys, zs))
+        out = np.zeros(len(s), dtype=np.float64)
+        assert self.lib.mcgpu_xperlin_sample_batch(_ptr(s), _ptr(x), _ptr(y), _ptr(z), len(s), _ptr(out)) == 0
+        return out

@@ -19,6 +19,9 @@ LIB = PKG / "libslime_b200.so"
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ["-std=c++17", "-O3", "-lineinfo", "-Xcompiler", "-fPIC,-O3", "-Xptxas", "-O3",
          "--expt-relaxed-constexpr"]
+# Per-file flags. The biome filter reproduces the reference's FP64/FP32 arithmetic operation by
+# operation, so neither the device nor the host compiler may contract a multiply and an add.
+FILE_FLAGS = {"biome.cu": ["--fmad=false", "-Xcompiler", "-ffp-contract=off"]}
 
 
 def nvcc() -> str:
@@ -49,7 +52,7 @@ def build(force: bool = False, verbose: bool = False) -> Path:
     jobs = []
     for src in sources():
         obj = objdir / (src.stem + ".o")
-        cmd = [nvcc(), *ARCH, *FLAGS, "-c", str(src), "-o", str(obj)]
+        cmd = [nvcc(), *ARCH, *FLAGS, *FILE_FLAGS.get(src.name, []), "-c", str(src), "-o", str(obj)]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         jobs.append((obj, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.PIPE, text=True)))

@@ -65,6 +65,32 @@ SIGNATURES = {
     "slime_b200_server_wait": (i32, [vp, i64, i32]),
     "slime_b200_server_take": (i64, [vp, i64, vp, i32, C.POINTER(C.c_double)]),
     "slime_b200_server_destroy": (None, [vp]),
+    # biome module (the reference's mcgpu_* C ABI, MinecraftGPUNoise.cu:1076-2018)
+    "mcgpu_api_version": (C.c_int, []),
+    "mcgpu_build_name": (C.c_char_p, []),
+    "mcgpu_modern_recommended_filter_batch": (i32, []),
+    "mcgpu_xoroshiro_nextlong_batch": (C.c_int, [vp, i32, i32, vp]),
+    "mcgpu_xperlin_sample_batch": (C.c_int, [vp, vp, vp, vp, i32, vp]),
+    "mcgpu_xperlin_sample_fixed_seed": (C.c_int, [C.c_uint64, vp, vp, vp, i32, vp]),
+    "mcgpu_continentalness_noise_fixed_seed": (C.c_int, [C.c_uint64, vp, vp, i32, vp]),
+    "mcgpu_climate5_fixed_seed": (C.c_int, [C.c_uint64, vp, vp, i32, vp]),
+    "mcgpu_climate5_quant_fixed_seed": (C.c_int, [C.c_uint64, vp, vp, i32, vp]),
+    "mcgpu_climate5_i32_fixed_seed": (C.c_int, [C.c_uint64, vp, vp, i32, vp]),
+    "mcgpu_climate_ctx_create": (vp, [C.c_uint64, i32]),
+    "mcgpu_climate_ctx_query_i32": (C.c_int, [vp, vp, vp, i32, vp]),
+    "mcgpu_climate_ctx_destroy": (None, [vp]),
+    "mcgpu_climate6_i32_fixed_seed": (C.c_int, [C.c_uint64, vp, vp, vp, i32, vp]),
+    "mcgpu_climate6_i32_fixed_seed_ex": (C.c_int, [C.c_uint64, i32, vp, vp, vp, i32, vp]),
+    "mcgpu_biome20_i32_fixed_seed": (C.c_int, [C.c_uint64, vp, vp, vp, i32, vp]),
+    "mcgpu_biome20_ctx_create": (vp, [C.c_uint64, i32]),
+    "mcgpu_biome20_ctx_query": (C.c_int, [vp, vp, vp, vp, i32, vp]),
+    "mcgpu_biome20_ctx_destroy": (None, [vp]),
+    "mcgpu_modern_ctx_create": (vp, [i32, C.c_uint64, i32]),
+    "mcgpu_modern_ctx_create_ex": (vp, [i32, C.c_uint64, i32, i32]),
+    "mcgpu_modern_ctx_query": (C.c_int, [vp, vp, vp, vp, i32, vp]),
+    "mcgpu_modern_ctx_filter_candidates": (C.c_int, [vp, vp, vp, i32, i32, vp]),
+    "mcgpu_modern_ctx_destroy": (None, [vp]),
+    "slime_b200_biome_last_stats": (None, [vp, C.POINTER(C.c_double), C.POINTER(i64)]),
 }
 
 # SlimeBatchRequest (48 bytes): the arguments of one search of a batch.
@@ -233,6 +259,57 @@ class SlimeServer:
     def close(self):
         if self.handle:
             self.lib.slime_b200_server_destroy(self.handle)
+            self.handle = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+
+def _i32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.int32)
+
+
+class BiomeFilter:
+    """A biome context of the C ABI (mcgpu_modern_ctx_*): one world seed, Minecraft version code
+    and biome size. filter() returns the Deep Dark (bit 0) / Mushroom Fields (bit 1) verdict mask
+    of candidate centre chunks, query() biome ids of quarts."""
+
+    def __init__(self, version: int, world_seed: int, capacity: int, large: int = 0,
+                 core: SlimeCoreB200 | None = None):
+        self.core = core or SlimeCoreB200()
+        self.lib = self.core.lib
+        self.capacity = capacity
+        self.handle = self.lib.mcgpu_modern_ctx_create_ex(version, world_seed & (2**64 - 1), large, capacity)
+        if not self.handle:
+            raise SlimeError("mcgpu_modern_ctx_create_ex failed: " + self.lib.slime_b200_last_error().decode())
+
+    def filter(self, cx, cz, flags: int = 3) -> np.ndarray:
+        x, z = _i32(cx), _i32(cz)
+        out = np.zeros(max(len(x), 1), dtype=np.int32)
+        rc = self.lib.mcgpu_modern_ctx_filter_candidates(self.handle, _ptr(x), _ptr(z), len(x), flags, _ptr(out))
+        if rc != 0:
+            raise SlimeError(f"filter_candidates: {rc} {self.lib.slime_b200_last_error().decode()}")
+        return out[: len(x)]
+
+    def query(self, xs, ys, zs) -> np.ndarray:
+        x, y, z = _i32(xs), _i32(ys), _i32(zs)
+        out = np.zeros(max(len(x), 1), dtype=np.int32)
+        rc = self.lib.mcgpu_modern_ctx_query(self.handle, _ptr(x), _ptr(y), _ptr(z), len(x), _ptr(out))
+        if rc != 0:
+            raise SlimeError(f"query: {rc} {self.lib.slime_b200_last_error().decode()}")
+        return out[: len(x)]
+
+    def last_stats(self):
+        ms, n = C.c_double(), C.c_int64()
+        self.lib.slime_b200_biome_last_stats(self.handle, C.byref(ms), C.byref(n))
+        return ms.value, n.value
+
+    def close(self):
+        if self.handle:
+            self.lib.mcgpu_modern_ctx_destroy(self.handle)
             self.handle = None
 
     def __enter__(self):
