@@ -178,9 +178,32 @@ int64_t slime_b200_search_noalloc(int64_t seed, int64_t rd_max, int32_t min_size
                                   int64_t rd_min, int32_t search_center_x, int32_t search_center_z,
                                   ExtChunkResult* results_buffer, int32_t max_results);
 
+/* ---- search with biome exclusion (replaces the search + mcgpu_modern_ctx_filter_candidates
+ *      round trip of the reference's frontend) ---------------------------------------------- */
+
+/* search_slime_clusters_gpu_v1_centered with the biome filter inside the call. biome_flags: bit 0
+ * exclude sites whose AFK window holds a slime chunk with a Deep Dark quart (quart Y -16..0),
+ * bit 1 one with a Mushroom Fields quart (quart Y 16), bit 2 large biomes; biome_version is the
+ * Minecraft version code of the parameter tree (>= 1194, e.g. 2602). The return value is still
+ * the number of centres in range (the filter does not change it); the results are the first
+ * min(passing, max_results) ranked sites whose verdict (mcgpu_modern_ctx_filter_candidates with
+ * the same flags) is 0, with precise scores of the best min(n, 100) when precise_afk != 0; the
+ * records after them, up to min(total, max_results), have size -1 (the same holds for the
+ * results of batches and of the server, whose requests carry the same flags). With
+ * biome_flags & 3 == 0 it is exactly search_slime_clusters_gpu_v1_centered. -1 on invalid
+ * arguments (including other flag bits or an unsupported version) or a CUDA failure. */
+int64_t slime_b200_search_biome(int64_t seed, int64_t rd_max, int32_t min_size, int32_t max_size,
+                                int64_t rd_min, int32_t search_center_x, int32_t search_center_z,
+                                ExtChunkResult* results_buffer, int32_t max_results, int32_t precise_afk,
+                                int32_t biome_flags, int32_t biome_version);
+
+/* Sites the biome filter examined and excluded in the last search (0 without a filter). */
+void slime_b200_last_biome_stats(int64_t* examined, int64_t* excluded);
+
 /* ---- batched search (no reference counterpart) --------------------------------------------- */
 
-/* One search of a batch: the arguments of search_slime_clusters_gpu_v1_centered. 48 bytes. */
+/* One search of a batch: the arguments of slime_b200_search_biome (those of
+ * search_slime_clusters_gpu_v1_centered plus the biome exclusion). 56 bytes. */
 typedef struct SlimeBatchRequest {
     int64_t seed;
     int64_t rd_max;
@@ -191,10 +214,12 @@ typedef struct SlimeBatchRequest {
     int32_t center_z;
     int32_t max_results;
     int32_t precise_afk;
+    int32_t biome_flags;    /* 0, or bit 0 exclude Deep Dark, bit 1 Mushroom Fields, bit 2 large biomes */
+    int32_t biome_version;  /* Minecraft version code of the biome tree, e.g. 2602 */
 } SlimeBatchRequest;
 
-/* Runs n searches as one batch. Searches with min_size >= 28 share one persistent launch of the
- * independent-band kernel whose CTAs take the tiles of all of them from one device queue; the
+/* Runs n searches as one batch (each with its own biome exclusion, as slime_b200_search_biome).
+ * Searches with min_size >= 28 share one persistent launch of the independent-band kernel whose CTAs take the tiles of all of them from one device queue; the
  * others (and any whose sites would not fit the batch's pool) run one by one. Request i writes
  * min(total_i, max_results_i) ranked results at results + (max_results_0 + ... +
  * max_results_{i-1}) and its total to totals[i], exactly as the single search would; totals[i]

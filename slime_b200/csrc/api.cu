@@ -65,6 +65,7 @@ bool Context::ensure_device() {
 void Context::release_extra() {}
 
 void Context::release() {
+    release_biome();
     xt.free();
     zt.free();
     hits.free();
@@ -352,6 +353,7 @@ int64_t Context::search(const SearchSpec& q, ExtChunkResult* results) {
     progress.store(1);
     last_kernel_ms = 0.0;
     last_launches = 0;
+    last_biome_examined = last_biome_excluded = 0;
     std::vector<Hit> best;
     std::vector<uint32_t> h(kHistBins, 0u);
     bool cancelled = false;
@@ -359,14 +361,74 @@ int64_t Context::search(const SearchSpec& q, ExtChunkResult* results) {
     const int32_t algo = engine_for(q);
     last_algorithm = algo;
     last_shape = algo == kAlgoBand ? 3 : algo == kAlgoIndep ? 4 : (2 * q.rd_max + 1) < 8192 ? 1 : 2;
-    if (!(algo == kAlgoGeneral ? scan_general(q, best, h, cancelled)
-                               : scan_band(q, best, h, cancelled, algo == kAlgoIndep))) {
-        progress.store(0);
-        return -1;
+    // With a biome exclusion the scan keeps more ranked sites than max_results (some fail the
+    // filter); when they run out before max_results pass, it runs again keeping four times more.
+    SearchSpec qs = q;
+    if (q.biome_flags & 3)
+        qs.max_results = (int32_t)std::min<int64_t>(INT32_MAX / 8, 2LL * q.max_results + 1024);
+    for (;;) {
+        if (!(algo == kAlgoGeneral ? scan_general(qs, best, h, cancelled)
+                                   : scan_band(qs, best, h, cancelled, algo == kAlgoIndep))) {
+            progress.store(0);
+            return -1;
+        }
+        const int64_t total = finish(q, best, h, results);
+        if (total == kNeedMoreSites && qs.max_results < INT32_MAX / 8) {
+            qs.max_results = (int32_t)std::min<int64_t>(INT32_MAX / 8, 4LL * qs.max_results);
+            best.clear();
+            std::fill(h.begin(), h.end(), 0u);
+            continue;
+        }
+        if (total < 0) progress.store(0);
+        else progress.store(90);
+        return total == kNeedMoreSites ? -1 : total;
     }
-    const int64_t total = finish(q, best, h, results);
-    if (total < 0) progress.store(0);
-    else progress.store(90);
+}
+
+// Biome exclusion after a scan: the ranked sites are filtered in rank order, a few thousand at a
+// time, until max_results pass (verdict mask & flags == 0) or the sites run out.
+int64_t Context::finish_biome(const SearchSpec& q, std::vector<Hit>& best, int64_t total, ExtChunkResult* results) {
+    std::sort(best.begin(), best.end(), hit_better);
+    const int32_t flags = q.biome_flags & 3, large = (q.biome_flags >> 2) & 1;
+    int32_t kept = 0;
+    size_t pos = 0;
+    std::vector<int32_t> cx, cz, mask;
+    while (kept < q.max_results && pos < best.size()) {
+        const size_t m = std::min(best.size() - pos, std::max<size_t>(4096, 2 * (size_t)(q.max_results - kept) + 256));
+        cx.resize(m);
+        cz.resize(m);
+        mask.resize(m);
+        for (size_t i = 0; i < m; ++i) {
+            cx[i] = best[pos + i].cx;
+            cz[i] = best[pos + i].cz;
+        }
+        if (!biome_masks(q.seed, q.biome_version, large, flags, cx.data(), cz.data(), (int64_t)m, mask.data()))
+            return -1;
+        for (size_t i = 0; i < m && kept < q.max_results; ++i) {
+            ++last_biome_examined;
+            if (mask[i] & flags) {
+                ++last_biome_excluded;
+                continue;
+            }
+            const Hit& b = best[pos + i];
+            ExtChunkResult& r = results[kept++];
+            r.size = b.count;
+            r.center_x = block_of(b.cx);
+            r.center_z = block_of(b.cz);
+            r.obs_count = 0;
+            r.afk_x = r.center_x;
+            r.afk_z = r.center_z;
+        }
+        pos += m;
+    }
+    if (kept < q.max_results && (int64_t)best.size() < total) return kNeedMoreSites;
+    // Records the exclusion left empty (up to the min(total, max_results) a caller expects)
+    // carry size -1.
+    for (int64_t i = kept; i < std::min<int64_t>(total, q.max_results); ++i)
+        results[i] = ExtChunkResult{-1, 0, 0, 0, 0, 0};
+    if (q.precise_afk && !cancel.load() && kept > 0) {
+        if (!score(q.seed, results, std::min(kept, 100), 1, y_enabled != 0)) return -1;
+    }
     return total;
 }
 
@@ -374,6 +436,7 @@ int64_t Context::finish(const SearchSpec& q, std::vector<Hit>& best, const std::
                         ExtChunkResult* results) {
     int64_t total = 0;
     for (int s = q.min_size; s <= q.max_size; ++s) total += h[s];
+    if (q.biome_flags & 3) return finish_biome(q, best, total, results);
     if (best.size() > (size_t)q.max_results)
         std::nth_element(best.begin(), best.begin() + q.max_results, best.end(), hit_better);
     const int32_t n = (int32_t)std::min<size_t>(best.size(), (size_t)q.max_results);
@@ -402,9 +465,10 @@ namespace {
 
 int64_t search_entry(int64_t seed, int64_t rd_max, int32_t min_size, int32_t max_size, int64_t rd_min,
                      int32_t cx, int32_t cz, ExtChunkResult* results, int32_t max_results,
-                     int32_t precise_afk) {
+                     int32_t precise_afk, int32_t biome_flags = 0, int32_t biome_version = 0) {
     std::lock_guard<std::mutex> lock(ctx().mu);
-    slime::SearchSpec q{seed, rd_max, min_size, max_size, rd_min, cx, cz, max_results, precise_afk};
+    slime::SearchSpec q{seed, rd_max, min_size, max_size, rd_min, cx, cz, max_results, precise_afk,
+                        biome_flags, biome_version};
     return ctx().search(q, reinterpret_cast<slime::ExtChunkResult*>(results));
 }
 
@@ -441,6 +505,20 @@ int64_t search_slime_clusters_gpu_v34_centered(int64_t seed, int64_t rd_max, int
     return search_slime_clusters_gpu_v1_centered(seed, rd_max, min_size, max_size, rd_min,
                                                  search_center_x, search_center_z, results_buffer,
                                                  max_results, precise_afk);
+}
+
+int64_t slime_b200_search_biome(int64_t seed, int64_t rd_max, int32_t min_size, int32_t max_size,
+                                int64_t rd_min, int32_t search_center_x, int32_t search_center_z,
+                                ExtChunkResult* results_buffer, int32_t max_results, int32_t precise_afk,
+                                int32_t biome_flags, int32_t biome_version) {
+    if ((biome_flags & ~7) != 0) return -1;
+    return search_entry(seed, rd_max, min_size, max_size, rd_min, search_center_x, search_center_z,
+                        results_buffer, max_results, precise_afk, biome_flags, biome_version);
+}
+
+void slime_b200_last_biome_stats(int64_t* examined, int64_t* excluded) {
+    if (examined) *examined = ctx().last_biome_examined;
+    if (excluded) *excluded = ctx().last_biome_excluded;
 }
 
 void refine_candidates_y(int64_t seed, ExtChunkResult* results_buffer, int32_t count) {
@@ -596,7 +674,7 @@ int32_t slime_b200_search_batch(const SlimeBatchRequest* requests, int32_t n, Ex
     for (int32_t i = 0; i < n; ++i) {
         const SlimeBatchRequest& r = requests[i];
         q[i] = slime::SearchSpec{r.seed, r.rd_max, r.min_size, r.max_size, r.rd_min, r.center_x, r.center_z,
-                                 r.max_results, r.precise_afk};
+                                 r.max_results, r.precise_afk, r.biome_flags, r.biome_version};
     }
     return ctx().search_batch(q.data(), n, reinterpret_cast<slime::ExtChunkResult*>(results), totals);
 }

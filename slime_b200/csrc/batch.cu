@@ -124,7 +124,7 @@ int32_t Context::search_batch(const SearchSpec* reqs, int32_t n, ExtChunkResult*
         const SearchSpec& q = reqs[i];
         totals[i] = -1;
         if (!validate_search(q.rd_max, q.min_size, q.max_size, q.rd_min, q.center_x, q.center_z,
-                             results + res_off[i], q.max_results))
+                             results + res_off[i], q.max_results) || (q.biome_flags & ~7) != 0)
             continue;
         // The batch takes what the single search would run on a band engine (whatever the
         // area's size: small areas fill the GPU together); the general scan's searches run alone.
@@ -301,6 +301,10 @@ int32_t Context::search_batch(const SearchSpec* reqs, int32_t n, ExtChunkResult*
                           flags_h[4 * s + 2], bt_counts.ptr + 2 * s + 1, bt_flags.ptr + 4 * s + 1, best, h))
             return -1;
         const int64_t total = finish(q, best, h, results + res_off[p.idx]);
+        if (total == kNeedMoreSites) {  // biome exclusion beyond the kept sites: run it alone
+            alone.push_back(p.idx);
+            continue;
+        }
         if (total < 0) return -1;
         totals[p.idx] = total;
         progress.store(1 + (int32_t)(80.0 * (s + 1) / std::max(1, m)));

@@ -125,12 +125,16 @@ float bits_to_float(int32_t b) {
     return f;
 }
 
+}  // namespace
+
 int tree_index(int32_t version) {
     int k = -1;
     for (int i = 0; i < BD_TREES; ++i)
         if (version >= BD_TREE[i].version_from) k = i;
     return k;
 }
+
+namespace {
 
 // Under the library lock, with the library's stream.
 bool ensure_tables() {
@@ -835,6 +839,31 @@ int perlin_host(const uint64_t* seeds, uint64_t fixed_seed, bool fixed, const do
 }
 
 }  // namespace biome
+
+namespace {
+biome::BiomeContext* g_search_ctx = nullptr;  // biome context of the last filtered search
+}
+
+bool biome_masks(int64_t world_seed, int32_t version, int32_t large, int32_t flags, const int32_t* cx,
+                 const int32_t* cz, int64_t n, int32_t* mask) {
+    if (n <= 0) return true;
+    biome::BiomeContext*& b = g_search_ctx;
+    if (!b || b->world_seed != (uint64_t)world_seed || b->version != version || b->large != (large ? 1 : 0)) {
+        biome::context_destroy(b);
+        b = biome::context_create(version, (uint64_t)world_seed, large, 1 << 18);
+        if (!b) {
+            if (biome::tree_index(version) < 0) ctx().set_error_text("biome filter: unsupported version code");
+            return false;
+        }
+    }
+    return biome::filter_host(b, cx, cz, n, flags, mask);
+}
+
+void release_biome() {
+    biome::context_destroy(g_search_ctx);
+    g_search_ctx = nullptr;
+}
+
 }  // namespace slime
 
 // ---- C ABI: the reference's biome module (MinecraftGPUNoise.cu:1076-2018) --------------------------

@@ -47,7 +47,12 @@ struct SearchSpec {
     int32_t center_z;
     int32_t max_results;
     int32_t precise_afk;
+    // Biome exclusion: bit 0 Deep Dark, bit 1 Mushroom Fields, bit 2 large biomes; 0 = none.
+    int32_t biome_flags = 0;
+    int32_t biome_version = 0;  // Minecraft version code of the biome tree (e.g. 2602)
 };
+
+constexpr int64_t kNeedMoreSites = -3;  // finish(): the biome exclusion needs more ranked sites
 
 // Values reported by get_gpu_v1_algorithm().
 constexpr int32_t kAlgoGeneral = 100;
@@ -159,9 +164,14 @@ struct Context {
                    bool& cancelled, bool indep);
     bool score(int64_t seed, ExtChunkResult* host, int32_t n, int32_t scan_xz, bool pack);
     int64_t search(const SearchSpec& q, ExtChunkResult* results);
-    // Total in range, ranked results and precise scores of a finished scan (-1 on failure).
+    // Total in range, ranked results and precise scores of a finished scan (-1 on failure). With
+    // a biome exclusion the results are the best sites whose window passes the filter; when
+    // fewer than max_results pass and `best` misses sites of the area, kNeedMoreSites.
     int64_t finish(const SearchSpec& q, std::vector<Hit>& best, const std::vector<uint32_t>& h,
                    ExtChunkResult* results);
+    int64_t finish_biome(const SearchSpec& q, std::vector<Hit>& best, int64_t total, ExtChunkResult* results);
+    // Sites examined and excluded by the biome filter in the last search.
+    int64_t last_biome_examined = 0, last_biome_excluded = 0;
     // Many searches: those the independent-band kernel can take share one persistent launch.
     int32_t search_batch(const SearchSpec* q, int32_t n, ExtChunkResult* results, int64_t* totals);
     // Sites and histogram of a finished band search from its emitted hits (already filtered
@@ -175,6 +185,13 @@ Context& ctx();
 
 // Forgets the cached device addresses of the no-alloc search's scratch array (noalloc.cu).
 void forget_noalloc_scratch();
+
+// Biome verdict masks (bit 0 Deep Dark, bit 1 Mushroom Fields) of n candidate centre chunks in
+// host memory, with a biome context of (world seed, version, large biomes) cached across calls
+// (biome.cu). Under the library lock. False on a CUDA failure or an unsupported version.
+bool biome_masks(int64_t world_seed, int32_t version, int32_t large, int32_t flags, const int32_t* cx,
+                 const int32_t* cz, int64_t n, int32_t* mask);
+void release_biome();
 
 // Sizing of per-search slices (batch.cu): the share of centres a threshold keeps in a window of
 // independent p = 0.1 cells, and the share of chunks that are rare redraw chunks.

@@ -192,7 +192,8 @@ bool Server::finish_band(Job* j) {
     if (!c.collect_band(j->q, j->area_x0, j->area_z0, hits_h.data(), n, j->rare, nrare, j->counts + 1, j->flags + 1,
                         best, h))
         return false;
-    const int64_t t = c.finish(j->q, best, h, j->results.data());
+    int64_t t = c.finish(j->q, best, h, j->results.data());
+    if (t == kNeedMoreSites) t = c.search(j->q, j->results.data());  // biome exclusion needs more sites
     if (t < 0) return false;
     j->total = t;
     return true;
@@ -362,11 +363,12 @@ int64_t slime_b200_server_submit(void* server, const SlimeBatchRequest* r) {
     if (!s || !r) return -1;
     auto j = std::make_unique<slime::Job>();
     j->q = slime::SearchSpec{r->seed, r->rd_max, r->min_size, r->max_size, r->rd_min, r->center_x, r->center_z,
-                             r->max_results, r->precise_afk};
+                             r->max_results, r->precise_afk, r->biome_flags, r->biome_version};
     std::vector<ExtChunkResult> probe(1);
     if (!slime::validate_search(j->q.rd_max, j->q.min_size, j->q.max_size, j->q.rd_min, j->q.center_x,
                                 j->q.center_z, reinterpret_cast<slime::ExtChunkResult*>(probe.data()),
-                                j->q.max_results))
+                                j->q.max_results) ||
+        (j->q.biome_flags & ~7) != 0)
         return -1;
     slime::plan_job(*j, slime::ctx());  // reads only the device's SM count and engine thresholds
     j->t_submit = std::chrono::steady_clock::now();

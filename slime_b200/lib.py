@@ -91,14 +91,17 @@ SIGNATURES = {
     "mcgpu_modern_ctx_filter_candidates": (C.c_int, [vp, vp, vp, i32, i32, vp]),
     "mcgpu_modern_ctx_destroy": (None, [vp]),
     "slime_b200_biome_last_stats": (None, [vp, C.POINTER(C.c_double), C.POINTER(i64)]),
+    "slime_b200_search_biome": (i64, [i64, i64, i32, i32, i64, i32, i32, vp, i32, i32, i32, i32]),
+    "slime_b200_last_biome_stats": (None, [C.POINTER(i64), C.POINTER(i64)]),
 }
 
-# SlimeBatchRequest (48 bytes): the arguments of one search of a batch.
+# SlimeBatchRequest (56 bytes): the arguments of one search of a batch.
 REQUEST_DTYPE = np.dtype(
     [("seed", "<i8"), ("rd_max", "<i8"), ("rd_min", "<i8"), ("min_size", "<i4"),
      ("max_size", "<i4"), ("center_x", "<i4"), ("center_z", "<i4"), ("max_results", "<i4"),
-     ("precise_afk", "<i4")]
+     ("precise_afk", "<i4"), ("biome_flags", "<i4"), ("biome_version", "<i4")]
 )
+assert REQUEST_DTYPE.itemsize == 56
 
 
 def load(path: Path | str = LIB) -> C.CDLL:
@@ -165,8 +168,7 @@ class SlimeCoreB200:
         list of (total, ranked results), one per search."""
         req = np.zeros(len(searches), dtype=REQUEST_DTYPE)
         for i, q in enumerate(searches):
-            req[i] = (q.seed, q.radius, q.rd_min, q.min_size, q.max_size, q.center_x, q.center_z,
-                      q.max_results, q.precise_afk)
+            req[i] = _request(q)[0]
         offs = np.concatenate([[0], np.cumsum(req["max_results"].astype(np.int64))])
         buf = np.zeros(max(int(offs[-1]), 1), dtype=RESULT_DTYPE)
         totals = np.zeros(max(len(searches), 1), dtype=np.int64)
@@ -176,8 +178,19 @@ class SlimeCoreB200:
         for i in range(len(searches)):
             t = int(totals[i])
             n = 0 if t < 0 else min(t, int(req["max_results"][i]))
-            out.append((t, buf[offs[i]:offs[i] + n].copy()))
+            out.append((t, passing(buf[offs[i]:offs[i] + n].copy())))
         return out
+
+    def search_biome(self, seed: int, rd_max: int, min_size: int, max_size: int = 221, rd_min: int = 0,
+                     center_x: int = 0, center_z: int = 0, max_results: int = 1000, precise_afk: int = 0,
+                     biome_flags: int = 3, biome_version: int = 2602):
+        """slime_b200_search_biome: the search with sites whose window holds Deep Dark (flag 1) /
+        Mushroom Fields (flag 2) excluded; returns (total, ranked results)."""
+        buf = np.zeros(max(max_results, 1), dtype=RESULT_DTYPE)
+        total = self.lib.slime_b200_search_biome(seed, rd_max, min_size, max_size, rd_min, center_x, center_z,
+                                                  _ptr(buf), max_results, precise_afk, biome_flags, biome_version)
+        self._check(total >= 0, "search_biome")
+        return total, passing(buf[: min(total, max_results)])
 
     def score_precise(self, seed: int, sites: np.ndarray, scan_xz: int = 1) -> np.ndarray:
         buf = np.ascontiguousarray(sites, dtype=RESULT_DTYPE).copy()
@@ -214,8 +227,9 @@ class SlimeCoreB200:
 
 def _request(q) -> np.ndarray:
     req = np.zeros(1, dtype=REQUEST_DTYPE)
+    flags = getattr(q, "biome_flags", 0)
     req[0] = (q.seed, q.radius, q.rd_min, q.min_size, q.max_size, q.center_x, q.center_z,
-              q.max_results, q.precise_afk)
+              q.max_results, q.precise_afk, flags, getattr(q, "biome_version", 2602) if flags else 0)
     return req
 
 
@@ -254,7 +268,7 @@ class SlimeServer:
         if total == -2:
             raise SlimeError(f"ticket {ticket} is not finished")
         n = 0 if total < 0 else min(total, max_results)
-        return total, buf[:n].copy(), lat.value
+        return total, passing(buf[:n].copy()), lat.value
 
     def close(self):
         if self.handle:
@@ -266,6 +280,12 @@ class SlimeServer:
 
     def __exit__(self, *exc):
         self.close()
+
+
+def passing(records: np.ndarray) -> np.ndarray:
+    """The records before the first with size -1 (the end of a biome-filtered result list)."""
+    end = np.flatnonzero(records["size"] < 0)
+    return records[: end[0]] if len(end) else records
 
 
 def _i32(a) -> np.ndarray:

@@ -34,6 +34,7 @@ class Search:
     max_results: int = 1000
     precise_afk: int = 0
     biome_flags: int = 0
+    biome_version: int = 2602   # Minecraft 26.2, the version of the reference's biome data
 
     @property
     def centres(self) -> int:

@@ -190,3 +190,82 @@ def test_query_and_climate_vs_reference_gpu(core, g):
     print(f"fmad build: {(c_f != o6).any(axis=1).sum()} of {n} quarts differ in a climate parameter, "
           f"{(b_f != ours).sum()} in the biome")
     assert (b_f != ours).sum() <= n // 1000
+
+
+def reference_filtered(q, ref_gpu_filter, pool=4000):
+    """The reference's answer to a biome-filtered search: its own search (reference CPU library up
+    to radius 20k, its GPU library above) keeping `pool` ranked sites, the reference biome filter
+    (sm_100a build, no contraction) on them, and the first max_results that pass."""
+    from dataclasses import replace
+    from tests.refcheck import reference_search
+    t, recs = reference_search(replace(q, max_results=pool, precise_afk=0))
+    cx = (recs["center_x"] - 8) // 16
+    cz = (recs["center_z"] - 8) // 16
+    mask = ref_gpu_filter.filter(q.biome_version, q.seed, cx, cz, q.biome_flags & 3, (q.biome_flags >> 2) & 1)
+    keep = recs[(mask & q.biome_flags & 3) == 0]
+    assert len(keep) >= min(q.max_results, t) or len(recs) == t
+    return t, keep[: q.max_results]
+
+
+def biome_searches():
+    from slime_b200.workloads import Search
+    return [
+        Search(seed=-7_123_456_789, center_x=0, center_z=0, radius=20_000, min_size=46, max_results=60, biome_flags=3),
+        Search(seed=424242, center_x=-600_000, center_z=350_000, radius=90_000, min_size=52, max_results=40,
+               biome_flags=1),
+        Search(seed=99, center_x=1_200_000, center_z=-10_000, radius=4_000, min_size=40, max_results=80,
+               biome_flags=2),
+        Search(seed=-31, center_x=5_000, center_z=5_000, radius=3_000, min_size=38, max_results=50,
+               biome_flags=3 | 4),
+        Search(seed=2024, center_x=0, center_z=0, radius=150_000, min_size=50, max_results=100, biome_flags=3,
+               biome_version=1215),
+    ]
+
+
+@pytest.mark.skipif(not REF_BIOME_GPU_SO["nofmad"].exists(), reason="reference biome build absent")
+def test_search_biome_vs_reference(core):
+    from oracle.oracle import RefBiomeGpu
+    ref = RefBiomeGpu("nofmad")
+    for q in biome_searches():
+        t, res = core.search_biome(q.seed, q.radius, q.min_size, q.max_size, q.rd_min, q.center_x, q.center_z,
+                                   q.max_results, 0, q.biome_flags, q.biome_version)
+        t_r, keep = reference_filtered(q, ref)
+        assert t == t_r, q
+        assert np.array_equal(res, keep), q
+    # Without flags it is the plain search.
+    q = biome_searches()[0]
+    a = core.search_biome(q.seed, q.radius, q.min_size, 221, 0, 0, 0, 500, 0, 0, 0)
+    b = core.search(q.seed, q.radius, q.min_size, 221, 0, 0, 0, 500, 0)
+    assert a[0] == b[0] and np.array_equal(a[1], b[1])
+
+
+def test_search_biome_precise_scores(core):
+    from tests.refcheck import ref_cpu
+    q = biome_searches()[0]
+    t, plain = core.search_biome(q.seed, q.radius, q.min_size, 221, 0, 0, 0, q.max_results, 0, 3, 2602)
+    t2, scored = core.search_biome(q.seed, q.radius, q.min_size, 221, 0, 0, 0, q.max_results, 1, 3, 2602)
+    assert t == t2 and np.array_equal(plain[["size", "center_x", "center_z"]], scored[["size", "center_x", "center_z"]])
+    assert np.array_equal(scored, ref_cpu().score_precise(q.seed, plain, scan_xz=1))
+
+
+def test_batch_and_server_biome_equal_single(core):
+    from slime_b200.lib import SlimeServer
+    qs = biome_searches()
+    singles = [core.search_biome(q.seed, q.radius, q.min_size, q.max_size, q.rd_min, q.center_x, q.center_z,
+                                 q.max_results, q.precise_afk, q.biome_flags, q.biome_version) for q in qs]
+    batch = core.search_batch(qs)
+    for (t, r), (tb, rb) in zip(singles, batch):
+        assert t == tb and np.array_equal(r, rb)
+    with SlimeServer(core=core) as server:
+        tickets = [server.submit(q) for q in qs]
+        for tk, q, (t, r) in zip(tickets, qs, singles):
+            assert server.wait(tk) == server.DONE
+            ts, rs, _ = server.take(tk, q.max_results)
+            assert ts == t and np.array_equal(rs, r)
+
+
+def test_search_biome_rejects_bad_flags(core):
+    from slime_b200.lib import RESULT_DTYPE
+    buf = np.zeros(4, dtype=RESULT_DTYPE)
+    assert core.lib.slime_b200_search_biome(1, 100, 40, 221, 0, 0, 0, _p(buf), 4, 0, 8, 2602) == -1
+    assert core.lib.slime_b200_search_biome(1, 100, 40, 221, 0, 0, 0, _p(buf), 4, 0, 3, 1100) == -1
