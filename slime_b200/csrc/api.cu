@@ -360,15 +360,19 @@ int64_t Context::search(const SearchSpec& q, ExtChunkResult* results) {
     last_rare = 0;
     const int32_t algo = engine_for(q);
     last_algorithm = algo;
-    last_shape = algo == kAlgoBand ? 3 : algo == kAlgoIndep ? 4 : (2 * q.rd_max + 1) < 8192 ? 1 : 2;
+    last_shape = algo == kAlgoBand || algo == kAlgoBandExact ? 3
+               : algo == kAlgoIndep || algo == kAlgoIndepExact ? 4
+               : (2 * q.rd_max + 1) < 8192 ? 1 : 2;
     // With a biome exclusion the scan keeps more ranked sites than max_results (some fail the
     // filter); when they run out before max_results pass, it runs again keeping four times more.
     SearchSpec qs = q;
     if (q.biome_flags & 3)
         qs.max_results = (int32_t)std::min<int64_t>(INT32_MAX / 8, 2LL * q.max_results + 1024);
     for (;;) {
+        const bool indep = algo == kAlgoIndep || algo == kAlgoIndepExact;
+        const bool exact = algo == kAlgoBandExact || algo == kAlgoIndepExact;
         if (!(algo == kAlgoGeneral ? scan_general(qs, best, h, cancelled)
-                                   : scan_band(qs, best, h, cancelled, algo == kAlgoIndep))) {
+                                   : scan_band(qs, best, h, cancelled, indep, exact))) {
             progress.store(0);
             return -1;
         }
@@ -630,7 +634,7 @@ void slime_b200_set_tuning(int32_t band_mad_add) {
 
 void slime_b200_set_engine(int32_t mode, int32_t band_min_threshold) {
     std::lock_guard<std::mutex> lock(ctx().mu);
-    ctx().engine_override = (mode >= 0 && mode <= 3) ? mode : 0;
+    ctx().engine_override = (mode >= 0 && mode <= 5) ? mode : 0;
     if (band_min_threshold >= 28 && band_min_threshold <= 221) ctx().band_min_threshold = band_min_threshold;
 }
 

@@ -39,6 +39,8 @@ bool Context::ensure_band() {
 // engine wants enough centres to fill the GPU. Below their thresholds the exact counts of the
 // many surviving 4x4 groups dominate and the general scan is faster.
 int32_t Context::engine_for(const SearchSpec& q) const {
+    if (engine_override == 4) return kAlgoBandExact;
+    if (engine_override == 5) return kAlgoIndepExact;
     if (engine_override == 1 || q.min_size < 28) return kAlgoGeneral;
     if (engine_override == 2) return kAlgoBand;
     if (engine_override == 3) return kAlgoIndep;
@@ -86,7 +88,7 @@ BandGeom band_geometry(int64_t W, int64_t H, bool indep, int sm_count) {
 }
 
 bool Context::scan_band(const SearchSpec& q, std::vector<Hit>& best, std::vector<uint32_t>& h,
-                        bool& cancelled, bool indep) {
+                        bool& cancelled, bool indep, bool exact) {
     if (!ensure_band()) return false;
     const int64_t W = 2 * q.rd_max + 1, H = W;
     const int32_t area_x0 = (int32_t)((int64_t)q.center_x - q.rd_max);
@@ -178,6 +180,7 @@ bool Context::scan_band(const SearchSpec& q, std::vector<Hit>& best, std::vector
             a.one = 1u;
             a.mad_add = band_mad_add;
             a.indep = indep ? 1 : 0;
+            a.exact = exact ? 1 : 0;
             a.row_stride = stride;
             const auto c0 = std::chrono::steady_clock::now();
             if ((e = cudaMemsetAsync(counters.ptr, 0, 8, stream)) != cudaSuccess ||
@@ -279,7 +282,7 @@ bool Context::scan_band(const SearchSpec& q, std::vector<Hit>& best, std::vector
         return false;
     }
     if (*(uint32_t*)pinned & 4u) { set_error("band engine: row-term copy timed out", cudaErrorLaunchTimeout); return false; }
-    if (*(uint32_t*)pinned) {
+    if (*(uint32_t*)pinned && !exact) {
         // A 4-row strip too dense for the byte-lane box: redo the search with the general scan.
         band_fallbacks++;
         std::fill(h.begin(), h.end(), 0u);

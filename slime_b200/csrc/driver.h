@@ -58,6 +58,9 @@ constexpr int64_t kNeedMoreSites = -3;  // finish(): the biome exclusion needs m
 constexpr int32_t kAlgoGeneral = 100;
 constexpr int32_t kAlgoBand = 200;
 constexpr int32_t kAlgoIndep = 300;
+// The band engines with bit-sliced exact counts of every centre (low thresholds).
+constexpr int32_t kAlgoBandExact = 210;
+constexpr int32_t kAlgoIndepExact = 310;
 
 constexpr size_t kPinnedBytes = 1 << 20;
 
@@ -114,7 +117,9 @@ struct Context {
     DeviceBuffer<BandArgs> bt_args;
     DeviceBuffer<int64_t> bt_prefix;
     bool band_ready = false;
-    int32_t engine_override = 0;       // 0 auto, 1 general scan, 2 band engine, 3 independent bands
+    // 0 auto, 1 general scan, 2 band engine, 3 independent bands, 4 / 5 the band / independent-band
+    // engine with bit-sliced exact counts.
+    int32_t engine_override = 0;
     // Engine rule (engine_for; slime_b200_set_engine_rule): the shared-LCG band engine for areas
     // at least band_min_periods periods wide from band_min_threshold, or band_fast_periods wide
     // from band_fast_threshold; independent bands for areas of indep_min_centres centres or more
@@ -161,7 +166,7 @@ struct Context {
     bool ensure_band();
     int32_t engine_for(const SearchSpec& q) const;
     bool scan_band(const SearchSpec& q, std::vector<Hit>& best, std::vector<uint32_t>& hist_out,
-                   bool& cancelled, bool indep);
+                   bool& cancelled, bool indep, bool exact = false);
     bool score(int64_t seed, ExtChunkResult* host, int32_t n, int32_t scan_xz, bool pack);
     int64_t search(const SearchSpec& q, ExtChunkResult* results);
     // Total in range, ranked results and precise scores of a finished scan (-1 on failure). With

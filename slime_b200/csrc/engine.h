@@ -88,6 +88,7 @@ struct BandArgs {
     uint32_t one;            // the value 1 (run time): band adds as multiply-adds when mad_add
     int32_t mad_add;
     int32_t indep;           // 1: independent bands (no shared LCG work, one X phase)
+    int32_t exact;           // 1: bit-sliced exact counts of every centre (no bounds)
     int64_t row_stride;      // input rows between band j and band j + 1 (2^17 with the shared LCG)
 };
 

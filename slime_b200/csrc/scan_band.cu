@@ -99,15 +99,21 @@ __device__ __forceinline__ bool bar_wait(unsigned long long* bar, uint32_t parit
     return false;
 }
 
-__device__ __forceinline__ uint32_t nibble_counts(uint32_t r) {
-    const uint32_t a = r - (__umulhi(r, 1u << 31) & 0x55555555u);
-    return (a & 0x33333333u) + (__umulhi(a, 1u << 30) & 0x33333333u);
+// Two-input add and subtract on the multiply pipe: `one` is 1 at run time, so the compiler emits
+// IMAD (the integer ALU pipe is the scan's bottleneck; the multiply pipe has room).
+__device__ __forceinline__ uint32_t madd(uint32_t a, uint32_t b, uint32_t one) { return a * one + b; }
+__device__ __forceinline__ uint32_t msub(uint32_t a, uint32_t b, uint32_t one) { return b * (0u - one) + a; }
+
+// Per nibble: the number of set bits (0..4). Shifts as multiply-highs, adds as multiply-adds.
+__device__ __forceinline__ uint32_t nibble_counts(uint32_t r, uint32_t one) {
+    const uint32_t a = msub(r, __umulhi(r, 1u << 31) & 0x55555555u, one);
+    return madd(a & 0x33333333u, __umulhi(a, 1u << 30) & 0x33333333u, one);
 }
 
 // Per byte: high bit set where v >= t (v, t < 256; borrow-free because v | 0x80 >= 128 >= t').
 // Bytes >= 128 always report (a superset is safe: flagged groups are re-tested).
-__device__ __forceinline__ uint32_t bytes_at_least(uint32_t v, uint32_t t4) {
-    return (((v | 0x80808080u) - t4) | v) & 0x80808080u;
+__device__ __forceinline__ uint32_t bytes_at_least(uint32_t v, uint32_t t4, uint32_t one) {
+    return (msub(v | 0x80808080u, t4, one) | v) & 0x80808080u;
 }
 
 struct Tile {
@@ -292,7 +298,7 @@ __device__ __forceinline__ void second_test(BandSmem& S, const BandArgs& a, cons
     const int r0 = 4 * (st - 4);  // rows 0 and 1 of strip st - 4
     uint32_t w0 = combo_word<kIndep>(S, r0, combo, fx, lane), w1 = combo_word<kIndep>(S, r0 + 1, combo, fx, lane);
     if (kMasked) { w0 &= cm; w1 &= cm; }
-    const uint32_t top01 = nibble_counts(w0) + nibble_counts(w1);
+    const uint32_t top01 = nibble_counts(w0, 1u) + nibble_counts(w1, 1u);
     // Outer cells of group g: 4-column blocks g and g + 4 of those four rows (byte lanes as in
     // the boxes: even groups from even blocks, odd groups from odd blocks).
     const uint32_t E = (top01 & 0x0F0F0F0Fu) + (n23 & 0x0F0F0F0Fu);
@@ -300,7 +306,7 @@ __device__ __forceinline__ void second_test(BandSmem& S, const BandArgs& a, cons
     // Lane 31 reads its own words here; only its groups 0..3 (which use no neighbour) can flag.
     const uint32_t En = __shfl_down_sync(kFull, E, 1), On = __shfl_down_sync(kFull, O, 1);
     const uint32_t oe = E + __funnelshift_r(E, En, 16), oo = O + __funnelshift_r(O, On, 16);
-    const uint32_t f2 = (bytes_at_least(re - oe, thr4) | (bytes_at_least(ro - oo, thr4) >> 1)) & flag;
+    const uint32_t f2 = (bytes_at_least(re - oe, thr4, 1u) | (bytes_at_least(ro - oo, thr4, 1u) >> 1)) & flag;
     uint32_t gm = 0;  // bit 8j+7 -> group 2j, bit 8j+6 -> group 2j+1
     for (uint32_t f = f2; f; f &= f - 1) {
         const int bit = __ffs(f) - 1;
@@ -353,7 +359,7 @@ template <bool kMasked, bool kIndep, bool kCands>
 __device__ __forceinline__ void count_strip(BandSmem& S, const BandArgs& a, const Tile& T, Counter& C,
                                             int slot, int t, int st, int warp, int lane, uint32_t fx,
                                             uint32_t lastmask, uint32_t thr4, uint32_t umask, uint32_t& guard,
-                                            int& ncand) {
+                                            int& ncand, uint32_t one) {
     const int r0 = 4 * t;  // t is a compile-time constant after unrolling
     const int hs = st % 5;
     const uint32_t live = st >= 4 ? lastmask : 0u;  // boxes are complete from the fifth strip on
@@ -373,25 +379,25 @@ __device__ __forceinline__ void count_strip(BandSmem& S, const BandArgs& a, cons
         for (int q = 0; q < 4; ++q) {
             uint32_t w = S.ring[slot][r0 + q][m][lane] & sel[q];
             if (kMasked) w &= C.cm[k];
-            n[q] = nibble_counts(w);
+            n[q] = nibble_counts(w, one);
         }
-        const uint32_t n01 = n[0] + n[1], n23 = n[2] + n[3];
-        const uint32_t e = (n01 & 0x0F0F0F0Fu) + (n23 & 0x0F0F0F0Fu);
-        const uint32_t o = ((n01 >> 4) & 0x0F0F0F0Fu) + ((n23 >> 4) & 0x0F0F0F0Fu);
+        const uint32_t n01 = madd(n[0], n[1], one), n23 = madd(n[2], n[3], one);
+        const uint32_t e = madd(n01 & 0x0F0F0F0Fu, n23 & 0x0F0F0F0Fu, one);
+        const uint32_t o = madd(__umulhi(n01, 1u << 28) & 0x0F0F0F0Fu, __umulhi(n23, 1u << 28) & 0x0F0F0F0Fu, one);
         // Lane 31 gets its own words back: they feed only groups 4..7, which it never flags.
         const uint32_t en = __shfl_down_sync(kFull, e, 1), on = __shfl_down_sync(kFull, o, 1);
-        const uint32_t s = e + o, sn = en + on;
+        const uint32_t s = madd(e, o, one), sn = madd(en, on, one);
         const uint32_t s1 = __funnelshift_r(s, sn, 8);
         const uint32_t ge = s + s1 + __funnelshift_r(e, en, 16);
         const uint32_t go = o + s1 + __funnelshift_r(s, sn, 16);
-        guard |= (ge + 0x4C4C4C4Cu) | (go + 0x4C4C4C4Cu);
+        guard |= madd(ge, 0x4C4C4C4Cu, one) | madd(go, 0x4C4C4C4Cu, one);
         uint32_t* he = &S.hist_e[hs][combo][lane];
         uint32_t* ho = &S.hist_o[hs][combo][lane];
-        C.re[k] += ge - *he;
-        C.ro[k] += go - *ho;
+        C.re[k] = madd(C.re[k], msub(ge, *he, one), one);
+        C.ro[k] = madd(C.ro[k], msub(go, *ho, one), one);
         *he = ge;
         *ho = go;
-        const uint32_t te = bytes_at_least(C.re[k], thr4), to = bytes_at_least(C.ro[k], thr4);
+        const uint32_t te = bytes_at_least(C.re[k], thr4, one), to = bytes_at_least(C.ro[k], thr4, one);
         fl[k] = (te | (to >> 1)) & live;  // even groups at bits 8j+7, odd groups at 8j+6
         n23s[k] = n23;
         any |= fl[k];
@@ -402,6 +408,238 @@ __device__ __forceinline__ void count_strip(BandSmem& S, const BandArgs& a, cons
             if (__any_sync(kFull, fl[k] != 0))
                 second_test<kMasked, kIndep, kCands>(S, a, T, fl[k], C.re[k], C.ro[k], n23s[k], kMasked ? C.cm[k] : ~0u,
                                              fx, thr4, warp + kWarps * k, lane, st, umask, warp, ncand);
+    }
+}
+
+// ---- exact counts of every centre, bit-sliced (low thresholds) ------------------------------
+//
+// Below a few units above the mean window count (22.1) most 4x4 groups pass every bound, and
+// counting each survivor with popcounts costs more than counting every centre exactly. This mode
+// does the latter with bit-sliced adders: a 32-bit word holds one bit of the counts of 32
+// consecutive centres (bit j = centre j of the lane's word), so a full adder over three words
+// (two LOP3) adds 32 centres' bits at once.
+//
+// For window rows i = 0..16 with half-widths h_i = 2,4,5,6,7,7,8,8,8,8,8,7,7,6,5,4,2, the cells at
+// horizontal offset k = |dx| from the centre column lie in the rows with h_i >= k, a contiguous
+// run of 17 (k <= 2), 15 (k = 3, 4), 13 (5), 11 (6), 9 (7) or 5 (8) rows. So the window count is
+//     sum over dx = -8..8 of V_{L(|dx|)}(column x + dx),
+// with V_L the vertical sum of the run of L rows, per column. The six V_L of a word's 32 columns are
+// built nested (V5 -> V9 -> ... -> V17, 43 LOP3), the next word's come by shuffle, and 17
+// funnel-shifted copies are added in a tree of ripple adders into 8 planes.
+
+__device__ __forceinline__ void bs_fa(uint32_t a, uint32_t b, uint32_t c, uint32_t& s, uint32_t& cy) {
+    s = a ^ b ^ c;
+    cy = (a & b) | (c & (a | b));
+}
+
+// out = a + b over NO planes (a: NA planes, b: NB <= NA planes; the caller knows the sum fits).
+template <int NA, int NB, int NO>
+__device__ __forceinline__ void bs_add(const uint32_t (&a)[NA], const uint32_t (&b)[NB], uint32_t (&out)[NO]) {
+    static_assert(NB <= NA && NO >= NA && NO <= NA + 1, "plane counts");
+    uint32_t c = 0;
+#pragma unroll
+    for (int i = 0; i < NA; ++i) {
+        if (i == 0) {
+            out[0] = a[0] ^ b[0];
+            c = a[0] & b[0];
+        } else if (i < NB) {
+            bs_fa(a[i], b[i], c, out[i], c);
+        } else {
+            out[i] = a[i] ^ c;
+            c = a[i] & c;
+        }
+    }
+    if constexpr (NO > NA) out[NA] = c;
+}
+
+// Copy of the N planes of v shifted right by dx within the 64-bit pair (own word, next word).
+template <int N>
+__device__ __forceinline__ void bs_shift(const uint32_t (&v)[N], const uint32_t (&vn)[N], int dx, uint32_t (&out)[N]) {
+#pragma unroll
+    for (int i = 0; i < N; ++i) out[i] = __funnelshift_r(v[i], vn[i], dx);
+}
+
+// Sum of the shifted copies at dx and 16 - dx of one vertical level.
+template <int N>
+__device__ __forceinline__ void bs_pair(const uint32_t (&v)[N], const uint32_t (&vn)[N], int dx, uint32_t (&out)[N + 1]) {
+    uint32_t a[N], b[N];
+    bs_shift<N>(v, vn, dx, a);
+    bs_shift<N>(v, vn, 16 - dx, b);
+    bs_add<N, N, N + 1>(a, b, out);
+}
+
+template <int N>
+__device__ __forceinline__ void bs_next(const uint32_t (&v)[N], uint32_t (&vn)[N]) {
+#pragma unroll
+    for (int i = 0; i < N; ++i) vn[i] = __shfl_down_sync(kFull, v[i], 1);
+}
+
+// Exact window counts (8 planes) of the 32 centres of the lane's word whose windows start at
+// row DZ of the 20 rows in R (window rows R[DZ] .. R[DZ + 16]).
+template <int DZ>
+__device__ __forceinline__ void bs_window_counts(const uint32_t (&Rr)[20], uint32_t (&cnt)[8]) {
+    const uint32_t* R = Rr + DZ;
+    // Vertical runs, nested: V5 = rows 6..10, V9 = 4..12, V11 = 3..13, V13 = 2..14, V15 = 1..15,
+    // V17 = 0..16.
+    uint32_t v5[3], v9[4], v11[4], v13[4], v15[4], v17[5];
+    {
+        uint32_t s1, c1, c2;
+        bs_fa(R[6], R[7], R[8], s1, c1);
+        bs_fa(R[9], R[10], s1, v5[0], c2);
+        v5[1] = c1 ^ c2;
+        v5[2] = c1 & c2;
+    }
+    {
+        uint32_t s, c, cc, c4;
+        bs_fa(R[4], R[5], R[11], s, c);
+        bs_fa(R[12], s, v5[0], v9[0], cc);
+        bs_fa(c, cc, v5[1], v9[1], c4);
+        v9[2] = c4 ^ v5[2];
+        v9[3] = c4 & v5[2];
+    }
+    auto add2 = [](const uint32_t (&v)[4], uint32_t x, uint32_t y, uint32_t (&o)[4]) {
+        uint32_t c;
+        bs_fa(x, y, v[0], o[0], c);
+        o[1] = v[1] ^ c; c &= v[1];
+        o[2] = v[2] ^ c; c &= v[2];
+        o[3] = v[3] ^ c;  // the sum stays below 16
+    };
+    add2(v9, R[3], R[13], v11);
+    add2(v11, R[2], R[14], v13);
+    add2(v13, R[1], R[15], v15);
+    {
+        uint32_t c;
+        bs_fa(R[0], R[16], v15[0], v17[0], c);
+        v17[1] = v15[1] ^ c; c &= v15[1];
+        v17[2] = v15[2] ^ c; c &= v15[2];
+        v17[3] = v15[3] ^ c; c &= v15[3];
+        v17[4] = c;
+    }
+    // The next word's levels (lane 31 gets its own back: only its centres 16+ would use them,
+    // and those lie beyond the tile's output columns).
+    uint32_t n5[3], n9[4], n11[4], n13[4], n15[4], n17[5];
+    bs_next<3>(v5, n5);
+    bs_next<4>(v9, n9);
+    bs_next<4>(v11, n11);
+    bs_next<4>(v13, n13);
+    bs_next<4>(v15, n15);
+    bs_next<5>(v17, n17);
+    // Horizontal: offsets dx = 0..16 from the window's first column; level by |dx - 8|.
+    uint32_t a1[4], a2[5], a3[5], a4[5], a5[5], a6[5], a7[6], a8[6], a9[5];
+    bs_pair<3>(v5, n5, 0, a1);      // dx 0, 16: max 10
+    bs_pair<4>(v9, n9, 1, a2);      // dx 1, 15: 18
+    bs_pair<4>(v11, n11, 2, a3);    // dx 2, 14: 22
+    bs_pair<4>(v13, n13, 3, a4);    // dx 3, 13: 26
+    bs_pair<4>(v15, n15, 4, a5);    // dx 4, 12: 30
+    bs_pair<4>(v15, n15, 5, a6);    // dx 5, 11: 30
+    bs_pair<5>(v17, n17, 6, a7);    // dx 6, 10: 34
+    bs_pair<5>(v17, n17, 7, a8);    // dx 7, 9: 34
+    bs_shift<5>(v17, n17, 8, a9);   // dx 8: 17
+    uint32_t b1[5], b2[6], b3[6], b4[7], c1[7], c2[8], d[8];
+    bs_add<5, 4, 5>(a2, a1, b1);    // 28
+    bs_add<5, 5, 6>(a3, a4, b2);    // 48
+    bs_add<5, 5, 6>(a5, a6, b3);    // 60
+    bs_add<6, 6, 7>(a7, a8, b4);    // 68
+    bs_add<6, 5, 7>(b2, b1, c1);    // 76
+    bs_add<7, 6, 8>(b4, b3, c2);    // 128
+    bs_add<8, 7, 8>(c2, c1, d);     // 204
+    bs_add<8, 5, 8>(d, a9, cnt);    // 221
+}
+
+// Centres whose count is at least t (t in 0..256): the carry out of count + (256 - t), with
+// the constant's bits known (one LOP3 per plane).
+__device__ __forceinline__ uint32_t bs_at_least(const uint32_t (&cnt)[8], int t) {
+    const uint32_t k = 256u - (uint32_t)t;
+    uint32_t c = 0;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) c = ((k >> b) & 1u) ? (cnt[b] | c) : (cnt[b] & c);
+    return (k & 256u) ? ~0u : c;
+}
+
+__device__ __forceinline__ int bs_value(const uint32_t (&cnt)[8], int j) {
+    int v = 0;
+#pragma unroll
+    for (int b = 0; b < 8; ++b) v |= (int)((cnt[b] >> j) & 1u) << b;
+    return v;
+}
+
+// Exact counts of strip st (window rows 4(st-4) .. 4st+3, centres of 4 rows) for the warp's
+// combos; centres in [min_size, max_size] (and outside the rd_min disc) are appended to the hit
+// list. Called by the whole warp; lane = word.
+template <bool kMasked, bool kIndep>
+__device__ __forceinline__ void exact_strip(const BandSmem& S, const BandArgs& a, const Tile& T, const Counter& C,
+                                            int st, int warp, int lane, uint32_t fx) {
+    constexpr int kUsed = kIndep ? kMaxBands / kWarps : kSlots;
+    const int r0 = 4 * (st - 4);
+    // Output columns of this word: centre index c = 32 lane + j < kOutW and inside the area.
+    const int64_t u_first = (int64_t)T.u0 + 32 * lane;
+#pragma unroll 1
+    for (int k = 0; k < kUsed; ++k) {
+        const int combo = warp + kWarps * k;
+        const int m = combo_band<kIndep>(combo), ph = combo_phase<kIndep>(combo);
+        if (m >= a.nb) continue;  // warp-uniform: planes of bands beyond the count are empty
+        uint32_t R[20];
+#pragma unroll
+        for (int i = 0; i < 20; ++i) {
+            uint32_t w = combo_word<kIndep>(S, r0 + i, combo, fx, lane);
+            if (kMasked) w &= C.cm[k];
+            R[i] = w;
+        }
+        // Columns of the word that are output centres of this combo.
+        uint32_t colok;
+        {
+            const int64_t ulim = min((int64_t)a.ubase, a.width_u - (int64_t)(T.i0 + ph) * kPeriod);
+            const int64_t nv = min(ulim - u_first, (int64_t)kOutW - 32 * lane);
+            colok = nv >= 32 ? ~0u : nv <= 0 ? 0u : (1u << nv) - 1u;
+        }
+        const int64_t band_v = (int64_t)(a.j0 + m) * a.row_stride;
+#pragma unroll
+        for (int dz = 0; dz < 4; ++dz) {
+            const int rr = r0 + dz;  // window start row = centre row index in the tile
+            const int64_t v = (int64_t)T.v0 + rr;
+            const bool rowok = rr < T.out_h && v + band_v < a.height_v;
+            uint32_t cnt[8];
+            if (dz == 0) bs_window_counts<0>(R, cnt);
+            else if (dz == 1) bs_window_counts<1>(R, cnt);
+            else if (dz == 2) bs_window_counts<2>(R, cnt);
+            else bs_window_counts<3>(R, cnt);
+            uint32_t pass = rowok ? colok & bs_at_least(cnt, a.min_size) : 0u;
+            if (a.max_size < 221) pass &= ~bs_at_least(cnt, a.max_size + 1);
+            if (!__any_sync(kFull, pass != 0)) continue;
+            // Append this lane's passing centres (outside the rd_min disc).
+            const int64_t cv = v + band_v;
+            uint32_t keep = 0;
+            for (uint32_t p = pass; p; p &= p - 1) {
+                const int j = __ffs(p) - 1;
+                if (a.rd_min_sq) {
+                    const int64_t cu = u_first + j + (int64_t)(T.i0 + ph) * kPeriod;
+                    const int32_t cx = (int32_t)(a.transposed ? a.area_x0 + cv : a.area_x0 + cu);
+                    const int32_t cz = (int32_t)(a.transposed ? a.area_z0 + cu : a.area_z0 + cv);
+                    const int64_t ddx = (int64_t)cx - a.center_x, ddz = (int64_t)cz - a.center_z;
+                    if (ddx * ddx + ddz * ddz < a.rd_min_sq) continue;
+                }
+                keep |= 1u << j;
+            }
+            const int n = __popc(keep);
+            int pos = n;
+#pragma unroll
+            for (int d2 = 1; d2 < 32; d2 <<= 1) {
+                const int t = __shfl_up_sync(kFull, pos, d2);
+                if (lane >= d2) pos += t;
+            }
+            const int total = __shfl_sync(kFull, pos, 31);
+            if (total == 0) continue;
+            unsigned long long base = 0;
+            if (lane == 31) base = atomicAdd(a.emitted, (unsigned long long)total);
+            base = __shfl_sync(kFull, base, 31) + (unsigned long long)(pos - n);
+            for (uint32_t p = keep; p; p &= p - 1, ++base) {
+                const int j = __ffs(p) - 1;
+                const int64_t cu = u_first + j + (int64_t)(T.i0 + ph) * kPeriod;
+                const int32_t cx = (int32_t)(a.transposed ? a.area_x0 + cv : a.area_x0 + cu);
+                const int32_t cz = (int32_t)(a.transposed ? a.area_z0 + cu : a.area_z0 + cv);
+                if (base < a.cap) a.out[base] = Hit{bs_value(cnt, j), cx, cz};
+            }
+        }
     }
 }
 
@@ -432,7 +670,7 @@ __device__ __forceinline__ void band_cta_init(BandSmem& S, int tid) {
 
 // One tile of one search (block-uniform arguments; all threads). Returns false when a bounded
 // wait gave up (the search's overflow word gets bit 4 and the CTA must stop).
-template <bool kMadAdd, bool kIndep, bool kCands>
+template <bool kMadAdd, bool kIndep, bool kCands, bool kExact = false>
 __device__ __forceinline__ bool band_tile(BandSmem& S, const BandArgs& a, int64_t tile, int tid, int lane,
                                           int warp, uint32_t& bar_phase) {
     const int nb = a.nb;
@@ -605,14 +843,23 @@ __device__ __forceinline__ bool band_tile(BandSmem& S, const BandArgs& a, int64_
                           kBatchBytes, &S.rows_bar[(b + 2) % 3]);
 
             // ---- counter: the two strips of batch b ------------------------------------------
+            if constexpr (kExact) {
+#pragma unroll
+                for (int t = 0; t < 2; ++t) {
+                    if (2 * b + t < 4) continue;  // windows complete from the fifth strip on
+                    if (interior) exact_strip<false, kIndep>(S, a, T, C, 2 * b + t, warp, lane, fx);
+                    else exact_strip<true, kIndep>(S, a, T, C, 2 * b + t, warp, lane, fx);
+                }
+                continue;
+            }
 #pragma unroll
             for (int t = 0; t < 2; ++t) {
                 if (interior)
                     count_strip<false, kIndep, kCands>(S, a, T, C, slot, t, 2 * b + t, warp, lane, fx, lastmask, thr4, umask,
-                                                       guard, ncand);
+                                                       guard, ncand, one);
                 else
                     count_strip<true, kIndep, kCands>(S, a, T, C, slot, t, 2 * b + t, warp, lane, fx, lastmask, thr4, umask,
-                                                      guard, ncand);
+                                                      guard, ncand, one);
             }
             // Candidates of this batch need rows of batches b-2..b, which stay in the ring until
             // batch b+2 is generated (after the next barrier).
@@ -633,7 +880,7 @@ __device__ __forceinline__ bool band_tile(BandSmem& S, const BandArgs& a, int64_
 // union counts per warp (kCands) pays; above it they are rare and are counted at once.
 constexpr int kCandThreshold = 56;
 
-template <bool kMadAdd, bool kIndep, bool kCands>
+template <bool kMadAdd, bool kIndep, bool kCands, bool kExact = false>
 __global__ void __launch_bounds__(kTpb, 1) band_scan_kernel(const BandArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     BandSmem& S = *reinterpret_cast<BandSmem*>(smem_raw);
@@ -642,7 +889,7 @@ __global__ void __launch_bounds__(kTpb, 1) band_scan_kernel(const BandArgs a) {
     uint32_t bar_phase = 0;  // bit r: parity of the next completion of rows_bar[r]
     band_cta_init(S, tid);
     for (int64_t tile = a.tile_begin + blockIdx.x; tile < a.tile_end; tile += gridDim.x)
-        if (!band_tile<kMadAdd, kIndep, kCands>(S, a, tile, tid, lane, warp, bar_phase)) return;
+        if (!band_tile<kMadAdd, kIndep, kCands, kExact>(S, a, tile, tid, lane, warp, bar_phase)) return;
 }
 
 // Many searches in one persistent launch (each search independent-band or shared-LCG): each CTA
@@ -759,10 +1006,10 @@ size_t band_smem_bytes() { return sizeof(BandSmem); }
 int band_tile_out_w() { return kOutW; }
 int band_max_bands() { return kMaxBands; }
 
-template <bool kMadAdd, bool kIndep, bool kCands>
+template <bool kMadAdd, bool kIndep, bool kCands, bool kExact = false>
 cudaError_t prepare_one(int bytes) {
-    return cudaFuncSetAttribute(band_scan_kernel<kMadAdd, kIndep, kCands>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                bytes);
+    return cudaFuncSetAttribute(band_scan_kernel<kMadAdd, kIndep, kCands, kExact>,
+                                cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
 cudaError_t band_prepare() {
@@ -772,6 +1019,8 @@ cudaError_t band_prepare() {
         (e = prepare_one<false, true, false>(bytes)) != cudaSuccess || (e = prepare_one<true, true, false>(bytes)) != cudaSuccess ||
         (e = prepare_one<false, false, true>(bytes)) != cudaSuccess || (e = prepare_one<true, false, true>(bytes)) != cudaSuccess ||
         (e = prepare_one<false, true, true>(bytes)) != cudaSuccess || (e = prepare_one<true, true, true>(bytes)) != cudaSuccess ||
+        (e = prepare_one<true, false, false, true>(bytes)) != cudaSuccess ||
+        (e = prepare_one<true, true, false, true>(bytes)) != cudaSuccess ||
         (e = cudaFuncSetAttribute(band_batch_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess)
         return e;
     return cudaFuncSetAttribute(band_batch_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
@@ -787,6 +1036,11 @@ cudaError_t launch_band_batch(const BandArgs* args, const int64_t* prefix, int32
 
 cudaError_t launch_band_scan(const BandArgs& a, int grid, cudaStream_t s) {
     const size_t bytes = sizeof(BandSmem);
+    if (a.exact) {  // bit-sliced exact counts of every centre (multiply-add band adds)
+        if (a.indep) band_scan_kernel<true, true, false, true><<<grid, kTpb, bytes, s>>>(a);
+        else band_scan_kernel<true, false, false, true><<<grid, kTpb, bytes, s>>>(a);
+        return cudaGetLastError();
+    }
     const bool cands = a.min_size < kCandThreshold;
     const int v = (a.mad_add ? 1 : 0) | (a.indep ? 2 : 0) | (cands ? 4 : 0);
     switch (v) {

@@ -66,24 +66,27 @@ def run(core, mode, *args, **kw):
         core.lib.slime_b200_set_engine(0, 0)
 
 
-# Engine modes: 2 = shared-LCG band engine, 3 = independent-band engine.
-ALGO = {2: 200, 3: 300}
+# Engine modes: 2 = shared-LCG band engine, 3 = independent-band engine, 4 / 5 = the same with
+# bit-sliced exact counts of every centre (any threshold).
+ALGO = {2: 200, 3: 300, 4: 210, 5: 310}
+MODES = [2, 3, 4, 5]
 
 
-@pytest.mark.parametrize("mode", [2, 3])
-@pytest.mark.parametrize("idx", [0, 1, 2, 7])
+@pytest.mark.parametrize("mode", MODES)
+@pytest.mark.parametrize("idx", range(8))
 def test_band_engine_search_golden(core, golden, idx, mode):
     g = golden["search"]
     name = str(g["names"][idx])
     seed, rd_max, lo, hi, rd_min, cx, cz, maxr, total = (int(v) for v in g["params"][idx])
-    assert lo >= 28
+    if mode in (2, 3) and lo < 28:
+        pytest.skip("the bounded band engines need a threshold of 28 or more")
     got_total, got = run(core, mode, seed, rd_max, lo, hi, rd_min, cx, cz, maxr)
     assert core.lib.get_gpu_v1_algorithm() == ALGO[mode]
     assert got_total == total, name
     assert np.array_equal(got, g[f"{name}_results"]), name
 
 
-@pytest.mark.parametrize("mode", [2, 3])
+@pytest.mark.parametrize("mode", MODES)
 @pytest.mark.parametrize("k,thr", [(0, 30), (1, 28), (2, 33), (3, 29)])
 def test_band_engine_planted_rare_chunk(core, oracle, k, thr, mode):
     x, z = 123_457 + 17 * k, -98_765 - 11 * k
@@ -100,7 +103,7 @@ def test_band_engine_planted_rare_chunk(core, oracle, k, thr, mode):
     assert t_g == t_o and np.array_equal(r_g, r_o)
 
 
-@pytest.mark.parametrize("mode", [2, 3])
+@pytest.mark.parametrize("mode", MODES)
 def test_band_engine_planted_rare_upper_bound(core, oracle, mode):
     x, z = -1_500_000, 1_400_000
     seed = rare_seed(x, z, 5)
@@ -110,7 +113,7 @@ def test_band_engine_planted_rare_upper_bound(core, oracle, mode):
     assert t_b == t_o and np.array_equal(r_b, r_o)
 
 
-@pytest.mark.parametrize("mode", [2, 3])
+@pytest.mark.parametrize("mode", MODES)
 @pytest.mark.parametrize("case", [
     (20240607, 140_000, 54, 221, 0, 0, 0, 2000),          # 2 phases x 3 bands, wide tiles
     (-31337, 300_000, 57, 221, 0, 400_000, -250_000, 500),  # 5 x 5 periods, offset centre
@@ -125,7 +128,7 @@ def test_band_vs_general_medium(core, case, mode):
     assert np.array_equal(r_b, r_g)
 
 
-@pytest.mark.parametrize("mode", [2, 3])
+@pytest.mark.parametrize("mode", MODES)
 def test_band_vs_general_low_threshold_millions_of_sites(core, mode):
     """Threshold 42 on a 280,001^2 area: 3.1 million sites, a survivor queue that overflows in
     every tile, and ~30 rare chunks whose distance test to far-away sites must not wrap."""
@@ -136,6 +139,20 @@ def test_band_vs_general_low_threshold_millions_of_sites(core, mode):
     t_b, r_b = run(core, mode, *case)
     assert t_g > 3_000_000
     assert core.lib.slime_b200_last_rare_chunks() > 0
+    assert t_b == t_g
+    assert np.array_equal(r_b, r_g)
+
+
+@pytest.mark.parametrize("mode", [4, 5])
+@pytest.mark.parametrize("case", [
+    (20240607, 140_000, 40, 221, 0, 0, 0, 2000),             # threshold 40, shared LCG: 2 x 3 bands
+    (-4242, 30_000, 36, 44, 5_000, 1_000_000, -3_000, 500),   # low threshold, upper bound, annulus
+    (123, 2_500, 25, 221, 0, 0, 0, 200_000),                  # below the bounded engines' range
+])
+def test_exact_counts_vs_general_low_thresholds(core, case, mode):
+    t_g, r_g = run(core, 1, *case)
+    t_b, r_b = run(core, mode, *case)
+    assert core.lib.get_gpu_v1_algorithm() == ALGO[mode]
     assert t_b == t_g
     assert np.array_equal(r_b, r_g)
 
