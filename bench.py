@@ -272,43 +272,72 @@ def run_other(args, rank=0, world=1, local_rank=0):
         return
 
     if args.workload == "precise":
-        # Full-world threshold-50 scans; every site gets its precise AFK score; the best 500 by
-        # (size, x, z) are kept. Biome exclusion is not built: the seeds run without it.
+        # Config 4: full-world threshold-50 scans; every site gets its precise AFK score; the
+        # biome filter (Deep Dark and Mushroom Fields excluded, Minecraft 26.2) runs over every
+        # site; the best 500 passing sites by (size, x, z) are kept.
+        from slime_b200.lib import BiomeFilter
         seeds = workloads.precise_biome_seeds()[: args.seeds]
         core.set_y_scan_config(0, -64, -64, 64, 4)
         cap = 2_000_000
         buf = np.zeros(cap, dtype=RESULT_DTYPE)
         sampler.start()
-        t_scan = t_prec = 0.0
-        sites = 0
+        t_scan = t_prec = t_bio = 0.0
+        bio_kernel_ms = 0.0
+        sites = excluded = unique = 0
         launches = 0
+        lazy_ms = []
         for q in seeds:
             core.lib.reset_cancel()
             t0 = time.perf_counter()
             total, res = core.search(q.seed, q.radius, q.min_size, q.max_size, 0, 0, 0, cap, 0, out=buf)
             t1 = time.perf_counter()
             scored = core.score_precise(q.seed, res, 1)
-            top = scored[: q.max_results]
             t2 = time.perf_counter()
-            assert total <= cap and len(top) == min(total, q.max_results)
+            cx = (scored["center_x"] - 8) // 16
+            cz = (scored["center_z"] - 8) // 16
+            with BiomeFilter(q.biome_version, q.seed, len(scored), core=core) as f:
+                mask = f.filter(cx, cz, q.biome_flags & 3)
+                kms, nu = f.last_stats()
+            top = scored[(mask & q.biome_flags & 3) == 0][: q.max_results]
+            t3 = time.perf_counter()
+            assert total <= cap and len(top) == min(q.max_results, int(((mask & 3) == 0).sum()))
             t_scan += t1 - t0
             t_prec += t2 - t1
+            t_bio += t3 - t2
+            bio_kernel_ms += kms
             sites += len(res)
-            launches += core.last_search_stats()[1] + 1
+            excluded += int(((mask & 3) != 0).sum())
+            unique += nu
+            launches += core.last_search_stats()[1] + 5
+            # The same answer through the one-call API (filter in rank order until 500 pass).
+            core.lib.reset_cancel()
+            t4 = time.perf_counter()
+            tl, lazy = core.search_biome(q.seed, q.radius, q.min_size, q.max_size, 0, 0, 0, q.max_results, 1,
+                                         q.biome_flags, q.biome_version)
+            lazy_ms.append((time.perf_counter() - t4) * 1e3)
+            assert tl == total and np.array_equal(lazy[["size", "center_x", "center_z"]],
+                                                  top[["size", "center_x", "center_z"]])
         sampler.stop()
         centres = sum(q.centres for q in seeds)
-        span = t_scan + t_prec
+        span = t_scan + t_prec + t_bio
         line.update({
-            "metric": "T centres/s full-world threshold-50 scan + precise scores of every site",
+            "metric": "T centres/s full-world threshold-50 scan + precise scores + biome filter of every site",
             "value": centres / span / 1e12, "unit": "T centres/s", "ms_per_step": span * 1e3 / len(seeds),
             "steps": len(seeds), "warmup": 0,
-            "e2e": {"value": centres / span / 1e12, "unit": "T centres/s", "h2d_bytes_per_step": 40 + 24 * sites // len(seeds),
-                    "d2h_bytes_per_step": 24 * 2 * sites // len(seeds)},
+            "e2e": {"value": centres / span / 1e12, "unit": "T centres/s",
+                    "h2d_bytes_per_step": 40 + 32 * sites // len(seeds),
+                    "d2h_bytes_per_step": (24 * 2 + 4) * sites // len(seeds)},
             "gpu_launches": launches,
             "config": {"workload": f"{len(seeds)} of the 16 seeds: radius 1,875,000, threshold 50, precise AFK score "
-                                   "(XZ scan, platform Y -64) of every site, top 500; biome exclusion not built",
-                       "sites_scored": sites, "scan_s": t_scan, "precise_s": t_prec,
+                                   "(XZ scan, platform Y -64) of every site, FP64 biome filter of every site "
+                                   "(Deep Dark and Mushroom Fields excluded, version 26.2), top 500 passing",
+                       "sites_scored": sites, "sites_excluded_by_biome": excluded,
+                       "unique_slime_chunks_evaluated": unique,
+                       "scan_s": t_scan, "precise_s": t_prec, "biome_s": t_bio,
+                       "biome_kernel_ms": bio_kernel_ms,
                        "precise_sites_per_s": sites / max(t_prec, 1e-9),
+                       "biome_sites_per_s": sites / max(t_bio, 1e-9),
+                       "one_call_ms_per_seed": lazy_ms,
                        "timing": "host wall clock around the C-ABI calls"},
             "clocks": sampler.summary(),
         })

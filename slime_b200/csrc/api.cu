@@ -641,10 +641,11 @@ void slime_b200_set_engine(int32_t mode, int32_t band_min_threshold) {
 const char* slime_b200_last_error(void) { return ctx().last_error; }
 
 int32_t slime_b200_set_engine_rule(const int64_t* rule, int32_t n) {
-    if (!rule || n != 6) return -1;
+    if (!rule || (n != 6 && n != 8)) return -1;
     const int64_t bt = rule[0], bp = rule[1], ft = rule[2], fp = rule[3], it = rule[4], ic = rule[5];
+    const int64_t et = n == 8 ? rule[6] : ctx().exact_below_threshold, ec = n == 8 ? rule[7] : ctx().exact_min_centres;
     if (bt < 28 || bt > 222 || ft < 28 || ft > 222 || it < 28 || it > 222 || bp < 2 || bp > 64 ||
-        fp < 2 || fp > 64 || ic < 0)
+        fp < 2 || fp > 64 || ic < 0 || et < 0 || et > 222 || ec < 0)
         return -1;
     std::lock_guard<std::mutex> lock(ctx().mu);
     slime::Context& c = ctx();
@@ -654,11 +655,13 @@ int32_t slime_b200_set_engine_rule(const int64_t* rule, int32_t n) {
     c.band_fast_periods = (int32_t)fp;
     c.indep_min_threshold = (int32_t)it;
     c.indep_min_centres = ic;
+    c.exact_below_threshold = (int32_t)et;
+    c.exact_min_centres = ec;
     return 0;
 }
 
 int32_t slime_b200_get_engine_rule(int64_t* rule, int32_t n) {
-    if (!rule || n != 6) return -1;
+    if (!rule || (n != 6 && n != 8)) return -1;
     std::lock_guard<std::mutex> lock(ctx().mu);
     const slime::Context& c = ctx();
     rule[0] = c.band_min_threshold;
@@ -667,6 +670,10 @@ int32_t slime_b200_get_engine_rule(int64_t* rule, int32_t n) {
     rule[3] = c.band_fast_periods;
     rule[4] = c.indep_min_threshold;
     rule[5] = c.indep_min_centres;
+    if (n == 8) {
+        rule[6] = c.exact_below_threshold;
+        rule[7] = c.exact_min_centres;
+    }
     return 0;
 }
 

@@ -48,6 +48,12 @@ int32_t Context::engine_for(const SearchSpec& q) const {
     // defaults are the B200 values). The shared LCG pays off with many periods (its work is
     // shared by every band and phase pair) and a high threshold.
     const int64_t w = 2 * q.rd_max + 1;
+    // Low thresholds: exact counts of every centre, while the sites stay few enough to collect
+    // (the band engines emit every site in range; the general scan gates by count on the device).
+    constexpr double kExactMaxSites = 1e9;
+    if (q.min_size < exact_below_threshold && w * w >= exact_min_centres &&
+        (double)w * (double)w * tail_share(q.min_size) <= kExactMaxSites)
+        return w >= (int64_t)band_fast_periods * kP ? kAlgoBandExact : kAlgoIndepExact;
     if ((q.min_size >= band_min_threshold && w >= (int64_t)band_min_periods * kP) ||
         (q.min_size >= band_fast_threshold && w >= (int64_t)band_fast_periods * kP))
         return kAlgoBand;

@@ -38,6 +38,7 @@ namespace {
 struct Planned {
     int32_t idx;          // request index
     BandGeom g;
+    bool exact;  // bit-sliced exact counts
     int32_t area_x0, area_z0;
     size_t ct_off, rt_off, hit_off, rare_off;
     uint64_t hit_cap;
@@ -129,7 +130,8 @@ int32_t Context::search_batch(const SearchSpec* reqs, int32_t n, ExtChunkResult*
         // The batch takes what the single search would run on a band engine (whatever the
         // area's size: small areas fill the GPU together); the general scan's searches run alone.
         const int32_t algo = engine_for(q);
-        const bool band_ok = q.min_size >= 28 && engine_override != 1 &&
+        const bool exact = algo == kAlgoBandExact || algo == kAlgoIndepExact;
+        const bool band_ok = (q.min_size >= 28 || exact) && engine_override != 1 &&
                              (algo != kAlgoGeneral || q.min_size >= indep_min_threshold);
         if (!band_ok) {
             alone.push_back(i);
@@ -137,8 +139,9 @@ int32_t Context::search_batch(const SearchSpec* reqs, int32_t n, ExtChunkResult*
         }
         Planned p{};
         p.idx = i;
+        p.exact = exact;
         const int64_t W = 2 * q.rd_max + 1;
-        p.g = band_geometry(W, W, algo != kAlgoBand, sm_count);
+        p.g = band_geometry(W, W, algo != kAlgoBand && algo != kAlgoBandExact, sm_count);
         p.area_x0 = (int32_t)((int64_t)q.center_x - q.rd_max);
         p.area_z0 = (int32_t)((int64_t)q.center_z - q.rd_max);
         const double centres = (double)W * (double)W;
@@ -214,6 +217,7 @@ int32_t Context::search_batch(const SearchSpec* reqs, int32_t n, ExtChunkResult*
             a.overflow = bt_flags.ptr + 4 * s;
             a.one = 1u;
             a.mad_add = band_mad_add;
+            a.exact = p.exact ? 1 : 0;
             a.indep = g.indep ? 1 : 0;
             a.row_stride = g.stride;
             prefix[s + 1] = prefix[s] + g.tiles;

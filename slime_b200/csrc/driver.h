@@ -131,6 +131,11 @@ struct Context {
     int32_t band_fast_periods = 4;
     int32_t indep_min_threshold = 42;
     int64_t indep_min_centres = 3600120001;
+    // Below exact_below_threshold, areas of exact_min_centres centres or more use the band engines
+    // with bit-sliced exact counts (shared LCG on areas band_fast_periods periods wide, else
+    // independent bands), as long as the expected number of sites stays below kExactMaxSites.
+    int32_t exact_below_threshold = 46;
+    int64_t exact_min_centres = 100000000;
     int64_t last_rare = 0;             // rare redraw chunks found by the last band search
     int64_t band_fallbacks = 0;        // band searches redone by the general scan
     int32_t band_mad_add = 1;          // generator variant: band adds on the multiply pipe

@@ -928,7 +928,15 @@ __global__ void __launch_bounds__(kTpb, 1) band_batch_kernel(const BandArgs* arg
             reinterpret_cast<uint32_t*>(&S.args)[i] = reinterpret_cast<const uint32_t*>(&args[s])[i];
         __syncthreads();
         bool ok;
-        if (S.args.indep) {
+        if (S.args.exact) {
+            // Exact counts read only the planes of the search's own bands.
+            if (S.args.indep)
+                ok = band_tile<kMadAdd, true, false, true>(S, S.args, S.args.tile_begin + t - prefix[s], tid, lane, warp,
+                                                           bar_phase);
+            else
+                ok = band_tile<kMadAdd, false, false, true>(S, S.args, S.args.tile_begin + t - prefix[s], tid, lane,
+                                                            warp, bar_phase);
+        } else if (S.args.indep) {
             ok = band_tile<kMadAdd, true, true>(S, S.args, S.args.tile_begin + t - prefix[s], tid, lane, warp, bar_phase);
         } else {
             // The shared-LCG counter reads every plane: clear planes of bands this search does

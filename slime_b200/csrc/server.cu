@@ -36,6 +36,7 @@ struct Job {
     SearchSpec q{};
     int32_t state = kQueued;
     bool band = false;        // runs in the batch kernel (else: the single search, whole)
+    bool exact = false;       // band work with bit-sliced exact counts
     bool started = false;
     Clock::time_point t_submit, t_done;
     int64_t total = -1;
@@ -92,13 +93,14 @@ void plan_job(Job& j, const Context& c) {
     const int32_t algo = c.engine_for(q);
     const double centres = (double)W * (double)W;
     const double expect = centres * tail_share(q.min_size);
-    j.band = q.min_size >= 28 && algo != kAlgoGeneral && expect * 1.5 < (double)(16u << 20);
+    j.exact = algo == kAlgoBandExact || algo == kAlgoIndepExact;
+    j.band = (q.min_size >= 28 || j.exact) && algo != kAlgoGeneral && expect * 1.5 < (double)(16u << 20);
     if (!j.band) {
         // The single search's term tables and hit buffer (library buffers, counted for gating).
         j.bytes = (size_t)(W + 16) * 16 + hit_capacity(q.max_results) * sizeof(Hit);
         return;
     }
-    j.g = band_geometry(W, W, algo != kAlgoBand, c.sm_count);
+    j.g = band_geometry(W, W, algo != kAlgoBand && algo != kAlgoBandExact, c.sm_count);
     j.area_x0 = (int32_t)((int64_t)q.center_x - q.rd_max);
     j.area_z0 = (int32_t)((int64_t)q.center_z - q.rd_max);
     j.hit_cap = (uint64_t)std::min<double>((double)(16u << 20), 2.0 * expect + 65536.0);
@@ -261,6 +263,7 @@ bool Server::step(std::vector<Job*>& live) {
         a.overflow = j->flags;
         a.one = 1u;
         a.mad_add = c.band_mad_add;
+        a.exact = j->exact ? 1 : 0;
         a.indep = g.indep ? 1 : 0;
         a.row_stride = g.stride;
         items.push_back(a);
