@@ -4,12 +4,14 @@
 
 For each (radius, threshold) point of a grid the search is timed with every engine that applies
 (the general scan, independent bands, and the shared-LCG band engine where the area spans two
-periods), forced through slime_b200_set_engine; every engine must return the same total and the
-same ranked sites. From the timings it derives the six numbers of slime_b200_set_engine_rule:
+periods, each of the band engines also with bit-sliced exact counts at low thresholds), forced
+through slime_b200_set_engine; every engine must return the same total and the same ranked sites.
+From the timings it derives the eight numbers of slime_b200_set_engine_rule:
 
   band_min_threshold, band_min_periods   shared LCG from this threshold on areas this many
   band_fast_threshold, band_fast_periods 2^17-chunk periods wide (two branches of the rule)
   indep_min_threshold, indep_min_centres independent bands instead of the general scan
+  exact_below_threshold, exact_min_centres  exact counts below this threshold on areas this large
 
 and writes them with the raw timings to a JSON file. SlimeCoreB200 applies that file when it
 loads the library. The general scan's rate does not depend on the area once it fills the GPU, so
@@ -42,18 +44,23 @@ def _time(core, mode, radius, thr, reps=2):
     return best, out
 
 
+EXACT_MAX_THRESHOLD = 50  # the exact modes are timed up to here (their cost does not depend on it)
+
+
 def measure(core, quick=False):
-    radii = [30_000, 100_000, 300_000, 600_000] + ([] if quick else [1_000_000])
+    radii = [10_000, 30_000, 100_000, 300_000, 600_000] + ([] if quick else [1_000_000])
     rows = []
     general_rate = {}
     for r in radii:
         w = 2 * r + 1
         for thr in range(40, 62, 4 if quick else 2):
-            if r >= 300_000 and thr < 42:
-                continue  # minutes of band work for no decision: the general scan wins there
             point = {"radius": r, "threshold": thr, "centres": w * w}
             ref = None
-            engines = [("indep", 3)] + ([("band", 2)] if w >= 2 * PERIOD else [])
+            engines = []
+            if thr >= 42 or r <= 100_000:
+                engines += [("indep", 3)] + ([("band", 2)] if w >= 2 * PERIOD else [])
+            if thr <= EXACT_MAX_THRESHOLD:
+                engines += [("indep_exact", 5)] + ([("band_exact", 4)] if w >= 2 * PERIOD else [])
             if r <= 100_000:
                 engines.insert(0, ("general", 1))
             for name, mode in engines:
@@ -67,6 +74,9 @@ def measure(core, quick=False):
                 general_rate[thr] = point["centres"] / point["general_s"]
             else:
                 point["general_s"] = point["centres"] / general_rate.get(thr, min(general_rate.values()))
+            for k in ("indep", "band"):  # bounded engines below 42 on large areas: never chosen
+                if k + "_s" not in point and (k == "indep" or w >= 2 * PERIOD):
+                    point[k + "_s"] = float("inf")
             rows.append(point)
     core.lib.slime_b200_set_engine(0, 0)
     return rows
@@ -114,7 +124,36 @@ def derive(rows):
         return total
 
     a, b = min(((x, y) for x in cands for y in cands), key=lambda ab: cost(*ab))
-    return [a[0], max(2, a[1]), b[0], max(2, b[1]), indep_min_threshold, indep_min_centres]
+    return [a[0], max(2, a[1]), b[0], max(2, b[1]), indep_min_threshold, indep_min_centres] + derive_exact(rows)
+
+
+def derive_exact(rows):
+    """exact_below_threshold: the exact modes take every threshold below it on the areas where
+    they win -- one above the highest threshold at which the best exact mode still beats every
+    other engine on all areas of at least exact_min_centres centres, the smallest measured area
+    where it wins at the lowest threshold."""
+    def exact_best(p):
+        return min(p[k] for k in ("indep_exact_s", "band_exact_s") if k in p)
+
+    def other_best(p):
+        return min(p[k] for k in ("general_s", "indep_s", "band_s") if k in p)
+
+    pts = [p for p in rows if "indep_exact_s" in p]
+    if not pts:
+        return [0, 1 << 62]
+    lowest = min(p["threshold"] for p in pts)
+    winners = sorted(p["centres"] for p in pts if p["threshold"] == lowest and exact_best(p) < other_best(p))
+    if not winners:
+        return [0, 1 << 62]
+    min_centres = winners[0]
+    below = 0
+    for thr in sorted({p["threshold"] for p in pts}):
+        big = [p for p in pts if p["threshold"] == thr and p["centres"] >= min_centres]
+        if big and all(exact_best(p) < other_best(p) for p in big):
+            below = thr + 1
+        else:
+            break
+    return [below, min_centres]
 
 
 def main():
@@ -133,7 +172,8 @@ def main():
     rule = derive(rows)
     doc = {"device": name.value.decode(errors="replace"),
            "rule": dict(zip(["band_min_threshold", "band_min_periods", "band_fast_threshold",
-                             "band_fast_periods", "indep_min_threshold", "indep_min_centres"], rule)),
+                             "band_fast_periods", "indep_min_threshold", "indep_min_centres",
+                             "exact_below_threshold", "exact_min_centres"], rule)),
            "seed": SEED, "max_results": 200, "points": rows}
     Path(args.out).write_text(json.dumps(doc, indent=1) + "\n")
     print(json.dumps(doc["rule"]))

@@ -205,12 +205,14 @@ bool Server::finish_band(Job* j) {
 bool Server::step(std::vector<Job*>& live) {
     Context& c = ctx();
     if (!c.ensure_device() || !c.ensure_band()) return false;
-    // Requests for the general scan run whole, one per step, first come first served.
-    for (Job* j : live) {
-        if (j->band) continue;
-        j->results.assign((size_t)std::max<int32_t>(1, j->q.max_results), ExtChunkResult{});
-        const int64_t t = c.search(j->q, j->results.data());
-        complete(j, t, t >= 0);
+    // Requests for the general scan run whole, one per step, the smallest area first.
+    Job* whole = nullptr;
+    for (Job* j : live)
+        if (!j->band && (!whole || j->q.rd_max < whole->q.rd_max)) whole = j;
+    if (whole) {
+        whole->results.assign((size_t)std::max<int32_t>(1, whole->q.max_results), ExtChunkResult{});
+        const int64_t t = c.search(whole->q, whole->results.data());
+        complete(whole, t, t >= 0);
         return true;
     }
     std::vector<Job*> band;
@@ -222,13 +224,20 @@ bool Server::step(std::vector<Job*>& live) {
         band.push_back(j);
     }
     if (band.empty()) return true;
-    // Work items: a quantum of tiles of every band job.
-    const int64_t quantum = std::max<int64_t>(c.sm_count, tiles_per_step / (int64_t)band.size());
+    // Work items, shortest remaining work first: each job in turn takes its remaining tiles up to
+    // what is left of the step's tile budget, and at least a floor of a quarter wave, so that
+    // small requests finish within a step while large ones keep moving.
+    std::sort(band.begin(), band.end(), [](const Job* x, const Job* y) {
+        return x->g.tiles - x->next_tile < y->g.tiles - y->next_tile;
+    });
+    const int64_t floor_tiles = std::max<int64_t>(1, c.sm_count / 4);
+    int64_t budget = tiles_per_step;
     std::vector<BandArgs> items;
     std::vector<int64_t> pre(1, 0);
     std::vector<int64_t> take;
     for (Job* j : band) {
-        const int64_t n = std::min<int64_t>(quantum, j->g.tiles - j->next_tile);
+        const int64_t n = std::min<int64_t>(std::max<int64_t>(budget, floor_tiles), j->g.tiles - j->next_tile);
+        budget = std::max<int64_t>(0, budget - n);
         take.push_back(n);
         if (n <= 0) continue;
         const SearchSpec& q = j->q;

@@ -18,7 +18,8 @@ def grid(indep_from, band_rule):
 def test_derive_recovers_the_crossovers():
     # Shared LCG wins from 48 on 9+ periods and from 54 on 4+ periods.
     rows = grid(44, lambda periods, thr: (periods >= 9 and thr >= 48) or (periods >= 4 and thr >= 54))
-    band_thr, band_periods, fast_thr, fast_periods, indep_thr, indep_centres = derive(rows)
+    band_thr, band_periods, fast_thr, fast_periods, indep_thr, indep_centres, ex_thr, ex_centres = derive(rows)
+    assert ex_thr == 0  # no exact timings: the exact modes are off
     assert indep_thr == 44 and indep_centres == (2 * 30_000 + 1) ** 2
     branches = {(band_thr, band_periods), (fast_thr, fast_periods)}
     assert branches == {(48, 9), (54, 4)}
@@ -31,3 +32,13 @@ def test_derive_never_picks_an_engine_that_loses_above_its_threshold():
         if p["threshold"] == 50:
             p["indep_s"] = 1.5
     assert derive(rows)[4] == 52
+
+
+def test_derive_exact_modes():
+    # Exact counts win below 46 on areas of 100k radius and more, and lose on the 30k area.
+    rows = grid(44, lambda periods, thr: periods >= 9 and thr >= 48)
+    for p in rows:
+        if p["threshold"] <= 50:
+            p["indep_exact_s"] = 0.1 if (p["threshold"] < 46 and p["radius"] >= 100_000) else 3.0
+    rule = derive(rows)
+    assert rule[6] == 45 and rule[7] == (2 * 100_000 + 1) ** 2  # wins at 44, loses at 46
