@@ -593,6 +593,17 @@ __device__ __forceinline__ void exact_strip(const BandSmem& S, const BandArgs& a
             colok = nv >= 32 ? ~0u : nv <= 0 ? 0u : (1u << nv) - 1u;
         }
         const int64_t band_v = (int64_t)(a.j0 + m) * a.row_stride;
+        // Annulus searches: skip the strip when all of its centres lie inside the rd_min disc
+        // (warp-uniform: the strip's 4 rows across the tile's output columns).
+        if (a.rd_min_sq) {
+            const int64_t u0 = (int64_t)T.u0 + (int64_t)(T.i0 + ph) * kPeriod, u1 = u0 + kOutW - 1;
+            const int64_t v0 = (int64_t)T.v0 + r0 + band_v, v1 = v0 + 3;
+            const int64_t x0 = a.transposed ? v0 : u0, x1 = a.transposed ? v1 : u1;
+            const int64_t z0 = a.transposed ? u0 : v0, z1 = a.transposed ? u1 : v1;
+            if (rect_inside_disc(a.area_x0 + x0, a.area_x0 + x1, a.area_z0 + z0, a.area_z0 + z1, a.center_x,
+                                 a.center_z, a.rd_min_sq))
+                continue;
+        }
 #pragma unroll
         for (int dz = 0; dz < 4; ++dz) {
             const int rr = r0 + dz;  // window start row = centre row index in the tile

@@ -93,6 +93,12 @@ __global__ void __launch_bounds__(TPB) general_scan_kernel(const ScanArgs a) {
         const int out_w = min(T::kOutW, a.width - x_base);
         const int out_h = min(a.band_h, a.slab_z0 + a.slab_h - z_base);
         const int in_w = out_w + 16, in_h = out_h + 16;
+        // Annulus searches: a tile whose centres all lie inside the rd_min disc keeps nothing
+        // (block-uniform; the farthest corner decides).
+        if (a.rd_min_sq && rect_inside_disc(a.area_x0 + (int64_t)x_base, a.area_x0 + (int64_t)x_base + out_w - 1,
+                                            a.area_z0 + (int64_t)z_base, a.area_z0 + (int64_t)z_base + out_h - 1,
+                                            a.center_x, a.center_z, a.rd_min_sq))
+            continue;
 
         uint64_t xt[CPT];
         int sq[CPT];

@@ -88,6 +88,16 @@ __host__ __device__ __forceinline__ bool slime_from_terms(uint64_t xt, uint64_t 
     return slime_redraw(state & kMask48);
 }
 
+// True when every centre of the rectangle [x0, x1] x [z0, z1] (chunk coordinates) lies strictly
+// inside the rd_min disc about (cx, cz), i.e. its farthest corner is closer than rd_min: an annulus
+// search keeps none of them.
+__host__ __device__ __forceinline__ bool rect_inside_disc(int64_t x0, int64_t x1, int64_t z0, int64_t z1, int64_t cx,
+                                                          int64_t cz, int64_t rd_min_sq) {
+    const int64_t dx = cx - x0 > x1 - cx ? cx - x0 : x1 - cx;
+    const int64_t dz = cz - z0 > z1 - cz ? cz - z0 : z1 - cz;
+    return dx * dx + dz * dz < rd_min_sq;
+}
+
 __host__ __device__ __forceinline__ bool is_slime(int64_t seed, int64_t x, int64_t z) {
     return slime_from_terms(x_term((int32_t)x), z_term((int32_t)z) + (uint64_t)seed);
 }

@@ -167,3 +167,19 @@ def test_band_full_world_vs_reference_gpu(core):
     t_r, r_r = RefGpu().search(spec.seed, spec.radius, 60, 221, 0, 0, 0, 1000)
     assert t_b == t_r
     assert np.array_equal(r_b, r_r)
+
+
+@pytest.mark.parametrize("mode", [1, 4, 5])
+@pytest.mark.parametrize("case", [
+    (2718281828, 20_000, 40, 221, 18_000, 250_000, -90_000, 3000),   # rd_min = 0.9 rd_max
+    (-161803, 6_000, 38, 45, 5_400, -1_000_000, 1_000_000, 800),     # with an upper bound
+])
+def test_annulus_skips_against_the_reference(core, case, mode):
+    """Tiles (general scan) and strips (exact counts) wholly inside the rd_min disc are skipped;
+    the result must still be the reference CPU library's."""
+    from slime_b200.workloads import Search
+    from tests.refcheck import check_against_reference
+    seed, r, lo, hi, rdm, cx, cz, maxr = case
+    total, res = run(core, mode, seed, r, lo, hi, rdm, cx, cz, maxr)
+    check_against_reference(Search(seed=seed, center_x=cx, center_z=cz, radius=r, min_size=lo, max_size=hi,
+                                   rd_min=rdm, max_results=maxr), total, res, f"annulus mode {mode}")
