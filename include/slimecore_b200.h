@@ -147,6 +147,13 @@ int32_t slime_b200_get_engine_rule(int64_t* rule, int32_t n);
  * per-band add on the multiply pipe instead of the integer ALU. */
 void slime_b200_set_tuning(int32_t band_mad_add);
 
+/* Polls of the band kernels' bounded mbarrier waits (row-term bulk copies) before a CTA gives up:
+ * it then waits, again bounded, for its copies still in flight, flags the search, and the search
+ * returns -1 with the error text "row-term copy timed out"; the library stays usable. polls < 0
+ * restores the default (2^22). Returns the previous value. For tests of that error path: with 0 the
+ * first wait gives up at once. */
+int64_t slime_b200_set_wait_limit(int64_t polls);
+
 /* Last CUDA error text of this library ("" if none). */
 const char* slime_b200_last_error(void);
 

@@ -632,6 +632,13 @@ void slime_b200_set_tuning(int32_t band_mad_add) {
     ctx().band_mad_add = band_mad_add ? 1 : 0;
 }
 
+int64_t slime_b200_set_wait_limit(int64_t polls) {
+    std::lock_guard<std::mutex> lock(ctx().mu);
+    const int64_t before = ctx().wait_polls;
+    ctx().wait_polls = polls < 0 ? (1u << 22) : (uint32_t)std::min<int64_t>(polls, UINT32_MAX);
+    return before;
+}
+
 void slime_b200_set_engine(int32_t mode, int32_t band_min_threshold) {
     std::lock_guard<std::mutex> lock(ctx().mu);
     ctx().engine_override = (mode >= 0 && mode <= 5) ? mode : 0;

@@ -187,6 +187,7 @@ bool Context::scan_band(const SearchSpec& q, std::vector<Hit>& best, std::vector
             a.mad_add = band_mad_add;
             a.indep = indep ? 1 : 0;
             a.exact = exact ? 1 : 0;
+            a.poll_limit = wait_polls;
             a.row_stride = stride;
             const auto c0 = std::chrono::steady_clock::now();
             if ((e = cudaMemsetAsync(counters.ptr, 0, 8, stream)) != cudaSuccess ||

@@ -218,6 +218,7 @@ int32_t Context::search_batch(const SearchSpec* reqs, int32_t n, ExtChunkResult*
             a.one = 1u;
             a.mad_add = band_mad_add;
             a.exact = p.exact ? 1 : 0;
+            a.poll_limit = wait_polls;
             a.indep = g.indep ? 1 : 0;
             a.row_stride = g.stride;
             prefix[s + 1] = prefix[s] + g.tiles;

@@ -139,6 +139,7 @@ struct Context {
     int64_t last_rare = 0;             // rare redraw chunks found by the last band search
     int64_t band_fallbacks = 0;        // band searches redone by the general scan
     int32_t band_mad_add = 1;          // generator variant: band adds on the multiply pipe
+    uint32_t wait_polls = 1u << 22;    // bounded mbarrier waits of the band kernels
 
     // Y-scan configuration (set_y_scan_config) and the tables built from it.
     int32_t y_enabled = 0, platform_y = -64, y_min = -64, y_max = 64, y_step = 4;

@@ -89,6 +89,7 @@ struct BandArgs {
     int32_t mad_add;
     int32_t indep;           // 1: independent bands (no shared LCG work, one X phase)
     int32_t exact;           // 1: bit-sliced exact counts of every centre (no bounds)
+    uint32_t poll_limit;     // polls of a row-term mbarrier before the CTA gives up (bit 4 of overflow)
     int64_t row_stride;      // input rows between band j and band j + 1 (2^17 with the shared LCG)
 };
 

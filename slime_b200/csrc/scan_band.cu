@@ -85,10 +85,10 @@ __device__ __forceinline__ void bulk_load(void* dst, const void* src, uint32_t b
                  :: "r"(smem_u32(dst)), "l"(src), "r"(bytes), "r"(smem_u32(bar)) : "memory");
 }
 
-// Waits for the mbarrier phase with the given parity; gives up after a bounded number of polls
-// and returns false (the caller flags an error instead of hanging the GPU).
-__device__ __forceinline__ bool bar_wait(unsigned long long* bar, uint32_t parity) {
-    for (int i = 0; i < (1 << 22); ++i) {
+// Waits for the mbarrier phase with the given parity; gives up after `polls` polls and returns
+// false (the caller flags an error instead of hanging the GPU).
+__device__ __forceinline__ bool bar_wait(unsigned long long* bar, uint32_t parity, uint32_t polls) {
+    for (uint32_t i = 0; i < polls; ++i) {
         uint32_t done;
         asm volatile("{ .reg .pred p;\n"
                      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n"
@@ -750,7 +750,7 @@ __device__ __forceinline__ bool band_tile(BandSmem& S, const BandArgs& a, int64_
         for (int b = 0; b < batches; ++b) {
             const int rb = b % 3, slot = b & (kRingSlots - 1);
             // ---- generator: batch b into ring slot b % 4 ------------------------------------
-            if (!bar_wait(&S.rows_bar[rb], (bar_phase >> rb) & 1u)) {
+            if (!bar_wait(&S.rows_bar[rb], (bar_phase >> rb) & 1u, a.poll_limit)) {
                 S.failed = 1;
                 if (lane == 0) atomicOr(a.overflow, 4u);
             }
@@ -846,7 +846,20 @@ __device__ __forceinline__ bool band_tile(BandSmem& S, const BandArgs& a, int64_
             }
             }
             __syncthreads();
-            if (S.failed) return false;  // block-uniform after the barrier
+            if (S.failed) {  // block-uniform after the barrier
+                // Before the CTA leaves, wait (bounded) for its row-term copies still in flight:
+                // batch b's (the wait that gave up) and batch b + 1's.
+                if (tid == 0) {
+                    constexpr uint32_t kDrainPolls = 1u << 22;
+                    bar_wait(&S.rows_bar[rb], ((bar_phase >> rb) & 1u) ^ 1u, kDrainPolls);
+                    if (b + 1 < batches) {
+                        const int rn = (b + 1) % 3;
+                        bar_wait(&S.rows_bar[rn], (bar_phase >> rn) & 1u, kDrainPolls);
+                    }
+                }
+                __syncthreads();
+                return false;
+            }
 
             // Row terms of batch b + 2 (its buffer was last read before this batch's barrier).
             if (tid == kTpb - 32 && b + 2 < batches)

@@ -273,6 +273,7 @@ bool Server::step(std::vector<Job*>& live) {
         a.one = 1u;
         a.mad_add = c.band_mad_add;
         a.exact = j->exact ? 1 : 0;
+        a.poll_limit = c.wait_polls;
         a.indep = g.indep ? 1 : 0;
         a.row_stride = g.stride;
         items.push_back(a);

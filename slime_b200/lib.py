@@ -54,6 +54,7 @@ SIGNATURES = {
     "slime_b200_last_rare_chunks": (i64, []),
     "slime_b200_set_engine": (None, [i32, i32]),
     "slime_b200_set_tuning": (None, [i32]),
+    "slime_b200_set_wait_limit": (i64, [i64]),
     "slime_b200_microbench": (i32, [i32, i32, C.POINTER(C.c_double), C.POINTER(C.c_double)]),
     "slime_b200_search_noalloc": (i64, [i64, i64, i32, i32, i64, i32, i32, vp, i32]),
     "slime_b200_search_batch": (i32, [vp, i32, vp, vp]),

@@ -183,3 +183,27 @@ def test_annulus_skips_against_the_reference(core, case, mode):
     total, res = run(core, mode, seed, r, lo, hi, rdm, cx, cz, maxr)
     check_against_reference(Search(seed=seed, center_x=cx, center_z=cz, radius=r, min_size=lo, max_size=hi,
                                    rd_min=rdm, max_results=maxr), total, res, f"annulus mode {mode}")
+
+
+@pytest.mark.parametrize("mode", [2, 3, 5])
+def test_bounded_wait_gives_up_cleanly(core, mode):
+    """With a poll limit of 0 the first row-term wait of every CTA gives up: the CTA drains its
+    copies in flight and flags the search, which returns -1 with an error text; with the default
+    limit restored the library searches as before (no GPU fault is involved)."""
+    case = (20240607, 140_000, 54, 221, 0, 0, 0, 2000)
+    t_ok, r_ok = run(core, 1, *case)
+    core.lib.slime_b200_set_wait_limit(0)
+    try:
+        core.lib.slime_b200_set_engine(mode, 0)
+        core.lib.reset_cancel()
+        buf = np.zeros(2000, dtype=r_ok.dtype)
+        import ctypes
+        total = core.lib.search_slime_clusters_gpu_v1_centered(*case[:7], buf.ctypes.data_as(ctypes.c_void_p),
+                                                               2000, 0)
+        assert total == -1
+        assert b"timed out" in core.lib.slime_b200_last_error()
+    finally:
+        core.lib.slime_b200_set_wait_limit(-1)
+        core.lib.slime_b200_set_engine(0, 0)
+    t_b, r_b = run(core, mode, *case)
+    assert t_b == t_ok and np.array_equal(r_b, r_ok)
