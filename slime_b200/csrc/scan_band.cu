@@ -54,6 +54,15 @@ template <bool kIndep>
 constexpr int row_words() { return kIndep ? kRowWordsI : kRowWords; }
 
 constexpr int kBatchRows = 8;               // rows per barrier: two 4-row strips
+// Generator layout: each lane evaluates bit `lane` of kGenW consecutive words (kGenW x 32 columns
+// per warp); kGenColWarps warps span the 32 words and each generates kGenRows rows of a batch.
+#ifndef SLIME_GEN_WORDS
+#define SLIME_GEN_WORDS 4
+#endif
+constexpr int kGenW = SLIME_GEN_WORDS;
+constexpr int kGenColWarps = 32 / kGenW;
+constexpr int kGenRows = kBatchRows / (16 / kGenColWarps);
+static_assert(kGenW % 4 == 0 && kGenRows >= 1, "generator layout");
 constexpr int kCandCap = 64;                // per warp: groups waiting for their union count
 constexpr int kRingSlots = 4;               // batches b-2..b are read while b+1 is generated
 
@@ -119,6 +128,16 @@ __device__ __forceinline__ uint32_t bytes_at_least(uint32_t v, uint32_t t4, uint
 struct Tile {
     int u0, v0, i0, out_h;
 };
+
+// The kGenW words of one plane at dst (16-byte aligned), as uint4 stores.
+__device__ __forceinline__ void store_plane(uint4* dst, const uint32_t (&w)[kGenW]) {
+#pragma unroll
+    for (int i = 0; i < kGenW / 4; ++i) dst[i] = make_uint4(w[4 * i], w[4 * i + 1], w[4 * i + 2], w[4 * i + 3]);
+}
+__device__ __forceinline__ void clear_plane(uint4* dst) {
+#pragma unroll
+    for (int i = 0; i < kGenW / 4; ++i) dst[i] = make_uint4(0u, 0u, 0u, 0u);
+}
 
 // Columns of word `word` that exist for phase `ph` of the tile (all ones inside the area).
 __device__ __forceinline__ uint32_t column_mask(const BandArgs& a, const Tile& T, int word, int ph) {
@@ -712,12 +731,12 @@ __device__ __forceinline__ bool band_tile(BandSmem& S, const BandArgs& a, int64_
         constexpr int kRW = row_words<kIndep>();
         constexpr uint32_t kBatchBytes = kBatchRows * kRW * 4;
 
-        // Generator columns of this thread: words 4*(warp%8) .. +3, lane = bit; the warp
-        // generates rows 4*(warp/8) .. +3 of every 8-row batch.
-        const int gw = (warp & 7) * 4, gq = (warp >> 3) * 4;
-        uint32_t lox[4], xh0[4], xh1[4];
+        // Generator columns of this thread: words kGenW*(warp % kGenColWarps) .. + kGenW - 1, lane =
+        // bit; the warp generates rows kGenRows*(warp / kGenColWarps) .. of every 8-row batch.
+        const int gw = (warp % kGenColWarps) * kGenW, gq = (warp / kGenColWarps) * kGenRows;
+        uint32_t lox[kGenW], xh0[kGenW], xh1[kGenW];
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
+        for (int k = 0; k < kGenW; ++k) {
             const int64_t idx0 = (int64_t)T.u0 + (gw + k) * 32 + lane + (int64_t)T.i0 * kPeriod;
             const uint64_t x0 = idx0 < a.ncols ? a.ct[idx0] : 0;
             const uint64_t x1 = idx0 + kPeriod < a.ncols ? a.ct[idx0 + kPeriod] : 0;
@@ -757,7 +776,7 @@ __device__ __forceinline__ bool band_tile(BandSmem& S, const BandArgs& a, int64_
             bar_phase ^= 1u << rb;
             if constexpr (kIndep) {
 #pragma unroll 1
-            for (int qq = 0; qq < 4; ++qq) {
+            for (int qq = 0; qq < kGenRows; ++qq) {
                 const int q = gq + qq;
                 const uint32_t* zr = &S.rows[rb][q * kRowWordsI];
                 const int nv = __shfl_sync(kFull, min((int)zr[kRowValidI], nb), 0);  // warp-uniform
@@ -767,28 +786,28 @@ __device__ __forceinline__ bool band_tile(BandSmem& S, const BandArgs& a, int64_
                 for (; m + 1 < nv; m += 2) {
                     const uint2 zh = *reinterpret_cast<const uint2*>(zr + m);
                     const uint2 zl = *reinterpret_cast<const uint2*>(zr + kRowLoI + m);
-                    uint32_t wa[4], wb[4];
+                    uint32_t wa[kGenW], wb[kGenW];
 #pragma unroll
-                    for (int k = 0; k < 4; ++k) {
+                    for (int k = 0; k < kGenW; ++k) {
                         wa[k] = __ballot_sync(kFull, indep_hit<kMadAdd>(lox[k], xh0[k], zl.x, zh.x, one));
                         wb[k] = __ballot_sync(kFull, indep_hit<kMadAdd>(lox[k], xh0[k], zl.y, zh.y, one));
                     }
-                    dst[m * kPlaneStep] = make_uint4(wa[0], wa[1], wa[2], wa[3]);
-                    dst[(m + 1) * kPlaneStep] = make_uint4(wb[0], wb[1], wb[2], wb[3]);
+                    store_plane(dst + m * kPlaneStep, wa);
+                    store_plane(dst + (m + 1) * kPlaneStep, wb);
                 }
                 if (m < nv) {
-                    uint32_t wa[4];
+                    uint32_t wa[kGenW];
 #pragma unroll
-                    for (int k = 0; k < 4; ++k)
+                    for (int k = 0; k < kGenW; ++k)
                         wa[k] = __ballot_sync(kFull, indep_hit<kMadAdd>(lox[k], xh0[k], zr[kRowLoI + m], zr[m], one));
-                    dst[m * kPlaneStep] = make_uint4(wa[0], wa[1], wa[2], wa[3]);
+                    store_plane(dst + m * kPlaneStep, wa);
                     ++m;
                 }
-                for (; m < nb; ++m) dst[m * kPlaneStep] = make_uint4(0u, 0u, 0u, 0u);  // rows outside band m
+                for (; m < nb; ++m) clear_plane(dst + m * kPlaneStep);  // rows outside band m
             }
             } else {
 #pragma unroll 1
-            for (int qq = 0; qq < 4; ++qq) {
+            for (int qq = 0; qq < kGenRows; ++qq) {
                 const int q = gq + qq;
                 const uint32_t* zr = &S.rows[rb][q * kRowWords];
                 const uint32_t zlo = zr[kRowLo];
@@ -796,9 +815,9 @@ __device__ __forceinline__ bool band_tile(BandSmem& S, const BandArgs& a, int64_
                 // (and the loops it bounds) is warp-uniform.
                 const int nv = __shfl_sync(kFull, min((int)zr[kRowValid], nb), 0);
                 const uint32_t zpar = (zr[0] ^ kXorHi) & 1u;
-                uint32_t xa[4], xb[4], dd[4], sw[4];
+                uint32_t xa[kGenW], xb[kGenW], dd[kGenW], sw[kGenW];
 #pragma unroll
-                for (int k = 0; k < 4; ++k) {
+                for (int k = 0; k < kGenW; ++k) {
                     const Shared sh = shared_part(lox[k], zlo);
                     const uint32_t pi = (sh.q0 ^ xh0[k] ^ sh.carry ^ zpar) & 1u;
                     xa[k] = (pi ? xh1[k] : xh0[k]) + sh.carry;
@@ -810,7 +829,7 @@ __device__ __forceinline__ bool band_tile(BandSmem& S, const BandArgs& a, int64_
                 // stores the same ballot words to the same address: no predicate, no branch.
                 uint4* dst = reinterpret_cast<uint4*>(&S.ring[slot][q][0][gw]);
                 constexpr int kPlaneStep = kWords / 4;  // uint4 per plane
-                dst[kSwPlane * kPlaneStep] = make_uint4(sw[0], sw[1], sw[2], sw[3]);
+                store_plane(dst + kSwPlane * kPlaneStep, sw);
                 auto hit = [&](uint32_t x, uint32_t z, uint32_t d) {
                     const uint32_t t = kMadAdd ? z * one + x : z + x;
                     return ((t ^ kXorHi) * kMulH + d) < kHitBelow;
@@ -820,28 +839,28 @@ __device__ __forceinline__ bool band_tile(BandSmem& S, const BandArgs& a, int64_
                     int m = 0;
                     for (; m + 1 < count; m += 2) {
                         const uint2 z2 = *reinterpret_cast<const uint2*>(zr + m);  // m even: aligned
-                        uint32_t wa[4], wb[4];
+                        uint32_t wa[kGenW], wb[kGenW];
 #pragma unroll
-                        for (int k = 0; k < 4; ++k) {
+                        for (int k = 0; k < kGenW; ++k) {
                             wa[k] = __ballot_sync(kFull, hit(xa[k], z2.x, dd[k]));
                             wb[k] = __ballot_sync(kFull, hit(xb[k], z2.y, dd[k]));
                         }
-                        dst[m * kPlaneStep] = make_uint4(wa[0], wa[1], wa[2], wa[3]);
-                        dst[(m + 1) * kPlaneStep] = make_uint4(wb[0], wb[1], wb[2], wb[3]);
+                        store_plane(dst + m * kPlaneStep, wa);
+                        store_plane(dst + (m + 1) * kPlaneStep, wb);
                     }
                     if (m < count) {  // odd count: the last band (m even) uses the even-band phase choice
                         const uint32_t z0 = zr[m];
-                        uint32_t wa[4];
+                        uint32_t wa[kGenW];
 #pragma unroll
-                        for (int k = 0; k < 4; ++k) wa[k] = __ballot_sync(kFull, hit(xa[k], z0, dd[k]));
-                        dst[m * kPlaneStep] = make_uint4(wa[0], wa[1], wa[2], wa[3]);
+                        for (int k = 0; k < kGenW; ++k) wa[k] = __ballot_sync(kFull, hit(xa[k], z0, dd[k]));
+                        store_plane(dst + m * kPlaneStep, wa);
                     }
                 };
                 if (nv == nb) {
                     bands(nb);  // the common case: the kernel-uniform band count bounds the loop
                 } else {
                     bands(nv);
-                    for (int m = nv; m < nb; ++m) dst[m * kPlaneStep] = make_uint4(0u, 0u, 0u, 0u);  // rows outside band m
+                    for (int m = nv; m < nb; ++m) clear_plane(dst + m * kPlaneStep);  // rows outside band m
                 }
             }
             }
