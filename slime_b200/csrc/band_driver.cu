@@ -139,164 +139,235 @@ bool Context::scan_band(const SearchSpec& q, std::vector<Hit>& best, std::vector
     const uint32_t nrare = *(uint32_t*)pinned;
     if (nrare > kRareCap) { set_error("too many rare chunks", cudaErrorMemoryAllocation); return false; }
     last_rare = nrare;
+    // The rare list sorted by x: the hit filter then binary-searches it.
+    if (nrare > 1) {
+        std::vector<int2> rl(nrare);
+        if ((e = cudaMemcpyAsync(rl.data(), rare.ptr, (size_t)nrare * sizeof(int2), cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
+            (e = cudaStreamSynchronize(stream)) != cudaSuccess) {
+            set_error("rare list", e);
+            return false;
+        }
+        std::sort(rl.begin(), rl.end(), [](const int2& a, const int2& b) { return a.x != b.x ? a.x < b.x : a.y < b.y; });
+        if ((e = cudaMemcpyAsync(rare.ptr, rl.data(), (size_t)nrare * sizeof(int2), cudaMemcpyHostToDevice, stream)) != cudaSuccess ||
+            (e = cudaStreamSynchronize(stream)) != cudaSuccess) {
+            set_error("rare list", e);
+            return false;
+        }
+    }
 
     const int64_t u_tiles = G.u_tiles, v_tiles = G.v_tiles;
     const int32_t band_h = G.band_h;
     const int grid = sm_count;
     const uint64_t cap = hits.count;
+    // Count histogram on the device (first-draw counts of every centre in range, corrected for
+    // rare chunks by the fix-up) and an emission gate: only centres whose count reaches emit_min
+    // are sent to the host, chosen so that the expected emission stays well inside the buffer but
+    // covers max_results several times; if it falls short, the scan runs again with the exact
+    // gate the histogram gives.
+    if ((e = hist.reserve(2 * kHistBins)) != cudaSuccess) { set_error("alloc", e); return false; }
+    unsigned int* dhist = hist.ptr;
+    int* ddelta = reinterpret_cast<int*>(hist.ptr + kHistBins);
+    const double area = (double)W * (double)H;
+    int32_t emit_min = q.min_size;
+    while (emit_min < q.max_size && area * tail_share(emit_min) > (double)cap / 8.0 &&
+           area * tail_share(emit_min + 1) >= 4.0 * q.max_results)
+        ++emit_min;
 
-    for (int64_t g = 0; g < ngroups; ++g) {
-        const int32_t j0 = (int32_t)(g * nb_max);
-        const int32_t nb = (int32_t)std::min<int64_t>(nb_max, nJ - j0);
-        if (nb <= 0) break;
-        const int64_t tiles = G.tiles;
-        int64_t chunk = std::max<int64_t>(grid, std::min<int64_t>(tiles, (int64_t)grid * 24));
-        for (int64_t t0 = 0; t0 < tiles;) {
-            while (paused.load() && !cancel.load()) std::this_thread::sleep_for(std::chrono::milliseconds(20));
-            if (cancel.load()) { cancelled = true; return true; }
-            const int64_t t1 = std::min(tiles, t0 + chunk);
-            BandArgs a{};
-            a.ct = xt.ptr;
-            a.ncols = width_u + 16;
-            a.rt = rt.ptr + (size_t)g * vrows_alloc * band_row_words(indep);
-            a.vrows = vrows;
-            a.vbase = vbase;
-            a.ubase = ubase;
-            a.width_u = width_u;
-            a.height_v = height_v;
-            a.j0 = j0;
-            a.nb = nb;
-            a.u_tiles = (int32_t)u_tiles;
-            a.v_tiles = (int32_t)v_tiles;
-            a.band_h = band_h;
-            a.tile_begin = t0;
-            a.tile_end = t1;
-            a.min_size = q.min_size;
-            a.max_size = q.max_size;
-            a.rd_min_sq = q.rd_min * q.rd_min;
-            a.area_x0 = area_x0;
-            a.area_z0 = area_z0;
-            a.center_x = q.center_x;
-            a.center_z = q.center_z;
-            a.transposed = transposed ? 1 : 0;
-            a.out = hits.ptr;
-            a.cap = cap;
-            a.emitted = counters.ptr;
-            a.overflow = flags.ptr;
-            a.one = 1u;
-            a.mad_add = band_mad_add;
-            a.indep = indep ? 1 : 0;
-            a.exact = exact ? 1 : 0;
-            a.poll_limit = wait_polls;
-            a.row_stride = stride;
-            const auto c0 = std::chrono::steady_clock::now();
-            if ((e = cudaMemsetAsync(counters.ptr, 0, 8, stream)) != cudaSuccess ||
-                (e = cudaEventRecord(ev_a, stream)) != cudaSuccess ||
-                (e = launch_band_scan(a, (int)std::min<int64_t>(grid, t1 - t0), stream)) != cudaSuccess ||
-                (e = cudaEventRecord(ev_b, stream)) != cudaSuccess ||
-                (e = cudaMemcpyAsync(pinned, counters.ptr, 8, cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
-                (e = cudaStreamSynchronize(stream)) != cudaSuccess) {
-                set_error("band scan", e);
-                return false;
-            }
-            const auto c1 = std::chrono::steady_clock::now();
-            float kms = 0.f;
-            cudaEventElapsedTime(&kms, ev_a, ev_b);
-            last_kernel_ms += kms;
-            ++last_launches;
-            const uint64_t emitted = *(unsigned long long*)pinned;
-            if (emitted > cap) {
-                if (t1 - t0 <= 1) { set_error("band hit buffer overflow", cudaErrorMemoryAllocation); return false; }
-                chunk = std::max<int64_t>(1, (t1 - t0) / 2);
-                continue;
-            }
-            work_ns.fetch_add(std::max<int64_t>(1, std::chrono::duration_cast<std::chrono::nanoseconds>(c1 - c0).count()));
-            if (emitted) {
-                if ((e = launch_filter_hits(hits.ptr, (int64_t)emitted, rare.ptr, (int32_t)nrare, stream)) != cudaSuccess) {
-                    set_error("filter", e);
+    for (int pass = 0; pass < 3; ++pass) {
+        best.clear();
+        std::fill(h.begin(), h.end(), 0u);
+        if ((e = cudaMemsetAsync(dhist, 0, 2 * kHistBins * sizeof(unsigned int), stream)) != cudaSuccess) {
+            set_error("band histogram", e);
+            return false;
+        }
+        for (int64_t g = 0; g < ngroups; ++g) {
+            const int32_t j0 = (int32_t)(g * nb_max);
+            const int32_t nb = (int32_t)std::min<int64_t>(nb_max, nJ - j0);
+            if (nb <= 0) break;
+            const int64_t tiles = G.tiles;
+            int64_t chunk = std::max<int64_t>(grid, std::min<int64_t>(tiles, (int64_t)grid * 24));
+            for (int64_t t0 = 0; t0 < tiles;) {
+                while (paused.load() && !cancel.load()) std::this_thread::sleep_for(std::chrono::milliseconds(20));
+                if (cancel.load()) { cancelled = true; return true; }
+                const int64_t t1 = std::min(tiles, t0 + chunk);
+                BandArgs a{};
+                a.ct = xt.ptr;
+                a.ncols = width_u + 16;
+                a.rt = rt.ptr + (size_t)g * vrows_alloc * band_row_words(indep);
+                a.vrows = vrows;
+                a.vbase = vbase;
+                a.ubase = ubase;
+                a.width_u = width_u;
+                a.height_v = height_v;
+                a.j0 = j0;
+                a.nb = nb;
+                a.u_tiles = (int32_t)u_tiles;
+                a.v_tiles = (int32_t)v_tiles;
+                a.band_h = band_h;
+                a.tile_begin = t0;
+                a.tile_end = t1;
+                a.min_size = q.min_size;
+                a.max_size = q.max_size;
+                a.rd_min_sq = q.rd_min * q.rd_min;
+                a.area_x0 = area_x0;
+                a.area_z0 = area_z0;
+                a.center_x = q.center_x;
+                a.center_z = q.center_z;
+                a.transposed = transposed ? 1 : 0;
+                a.out = hits.ptr;
+                a.cap = cap;
+                a.emitted = counters.ptr;
+                a.overflow = flags.ptr;
+                a.one = 1u;
+                a.mad_add = band_mad_add;
+                a.indep = indep ? 1 : 0;
+                a.exact = exact ? 1 : 0;
+                a.poll_limit = wait_polls;
+                a.hist = dhist;
+                a.emit_min = emit_min;
+                a.row_stride = stride;
+                const auto c0 = std::chrono::steady_clock::now();
+                // A launch whose hits overflow the buffer is redone in halves: its histogram
+                // counts are taken back first (snapshot before, restore after).
+                if ((e = cudaMemcpyAsync(ddelta, dhist, kHistBins * sizeof(unsigned int), cudaMemcpyDeviceToDevice,
+                                         stream)) != cudaSuccess ||
+                    (e = cudaMemsetAsync(counters.ptr, 0, 8, stream)) != cudaSuccess ||
+                    (e = cudaEventRecord(ev_a, stream)) != cudaSuccess ||
+                    (e = launch_band_scan(a, (int)std::min<int64_t>(grid, t1 - t0), stream)) != cudaSuccess ||
+                    (e = cudaEventRecord(ev_b, stream)) != cudaSuccess ||
+                    (e = cudaMemcpyAsync(pinned, counters.ptr, 8, cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
+                    (e = cudaStreamSynchronize(stream)) != cudaSuccess) {
+                    set_error("band scan", e);
                     return false;
                 }
-                if (nrare) ++last_launches;
+                const auto c1 = std::chrono::steady_clock::now();
+                float kms = 0.f;
+                cudaEventElapsedTime(&kms, ev_a, ev_b);
+                last_kernel_ms += kms;
+                ++last_launches;
+                const uint64_t emitted = *(unsigned long long*)pinned;
+                if (emitted > cap) {
+                    if (t1 - t0 <= 1) { set_error("band hit buffer overflow", cudaErrorMemoryAllocation); return false; }
+                    if ((e = cudaMemcpyAsync(dhist, ddelta, kHistBins * sizeof(unsigned int), cudaMemcpyDeviceToDevice,
+                                             stream)) != cudaSuccess) {
+                        set_error("band histogram", e);
+                        return false;
+                    }
+                    chunk = std::max<int64_t>(1, (t1 - t0) / 2);
+                    continue;
+                }
+                work_ns.fetch_add(std::max<int64_t>(1, std::chrono::duration_cast<std::chrono::nanoseconds>(c1 - c0).count()));
+                if (emitted) {
+                    if ((e = launch_filter_hits(hits.ptr, (int64_t)emitted, rare.ptr, (int32_t)nrare, true, stream)) != cudaSuccess) {
+                        set_error("filter", e);
+                        return false;
+                    }
+                    if (nrare) ++last_launches;
+                    const size_t old = best.size();
+                    best.resize(old + emitted);
+                    if ((e = cudaMemcpyAsync(best.data() + old, hits.ptr, emitted * sizeof(Hit), cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
+                        (e = cudaStreamSynchronize(stream)) != cudaSuccess) {
+                        set_error("copy", e);
+                        return false;
+                    }
+                    size_t w = old;
+                    for (size_t i = old; i < best.size(); ++i)
+                        if (best[i].count >= 0) best[w++] = best[i];  // window holds a rare chunk: fixed below
+                    best.resize(w);
+                    if (best.size() > 2 * (size_t)q.max_results + 1000000) {
+                        std::nth_element(best.begin(), best.begin() + q.max_results, best.end(),
+                                         [](const Hit& x, const Hit& y) { return hit_order(x, y); });
+                        best.resize(q.max_results);
+                    }
+                }
+                const double done = ((double)g * tiles + (double)t1) / ((double)ngroups * tiles);
+                processed.store((int64_t)(done * (double)W * (double)H));
+                progress.store(1 + (int32_t)(done * 78));
+                t0 = t1;
+            }
+        }
+
+        // Exact counts of every centre whose window holds a rare redraw chunk, and the matching
+        // correction of the histogram (first-draw count out, exact count in).
+        if ((e = cudaMemsetAsync(ddelta, 0, kHistBins * sizeof(int), stream)) != cudaSuccess) {
+            set_error("band histogram", e);
+            return false;
+        }
+        if (nrare) {
+            FixArgs f{};
+            f.area_x0 = area_x0;
+            f.area_z0 = area_z0;
+            f.width = W;
+            f.height = H;
+            f.rd_min_sq = q.rd_min * q.rd_min;
+            f.center_x = q.center_x;
+            f.center_z = q.center_z;
+            f.min_size = q.min_size;
+            f.max_size = q.max_size;
+            f.fixed = fixed.ptr;
+            f.fixed_count = counters.ptr + 1;
+            f.cap = fixed.count;
+            f.error = flags.ptr + 1;
+            f.hist_delta = ddelta;
+            if ((e = cudaMemsetAsync(counters.ptr + 1, 0, 8, stream)) != cudaSuccess ||
+                (e = launch_fixup(rare.ptr, (int32_t)nrare, q.seed, f, stream)) != cudaSuccess ||
+                (e = cudaMemcpyAsync(pinned, counters.ptr + 1, 8, cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
+                (e = cudaMemcpyAsync((char*)pinned + 8, flags.ptr, 8, cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
+                (e = cudaStreamSynchronize(stream)) != cudaSuccess) {
+                set_error("fixup", e);
+                return false;
+            }
+            ++last_launches;
+            const uint64_t nf = *(unsigned long long*)pinned;
+            const uint32_t* fl = (const uint32_t*)((char*)pinned + 8);
+            if (nf > fixed.count || fl[1]) { set_error("fixup overflow", cudaErrorUnknown); return false; }
+            if (nf) {
                 const size_t old = best.size();
-                best.resize(old + emitted);
-                if ((e = cudaMemcpyAsync(best.data() + old, hits.ptr, emitted * sizeof(Hit), cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
+                best.resize(old + nf);
+                if ((e = cudaMemcpyAsync(best.data() + old, fixed.ptr, nf * sizeof(Hit), cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
                     (e = cudaStreamSynchronize(stream)) != cudaSuccess) {
                     set_error("copy", e);
                     return false;
                 }
-                size_t w = old;
-                for (size_t i = old; i < best.size(); ++i) {
-                    if (best[i].count < 0) continue;  // window holds a rare chunk: fixed below
-                    ++h[best[i].count];
-                    best[w++] = best[i];
-                }
-                best.resize(w);
-                if (best.size() > 2 * (size_t)q.max_results + 1000000) {
-                    std::nth_element(best.begin(), best.begin() + q.max_results, best.end(),
-                                     [](const Hit& x, const Hit& y) { return hit_order(x, y); });
-                    best.resize(q.max_results);
-                }
             }
-            const double done = ((double)g * tiles + (double)t1) / ((double)ngroups * tiles);
-            processed.store((int64_t)(done * (double)W * (double)H));
-            progress.store(1 + (int32_t)(done * 78));
-            t0 = t1;
         }
-    }
-
-    // Exact counts of every centre whose window holds a rare redraw chunk.
-    if (nrare) {
-        FixArgs f{};
-        f.area_x0 = area_x0;
-        f.area_z0 = area_z0;
-        f.width = W;
-        f.height = H;
-        f.rd_min_sq = q.rd_min * q.rd_min;
-        f.center_x = q.center_x;
-        f.center_z = q.center_z;
-        f.min_size = q.min_size;
-        f.max_size = q.max_size;
-        f.fixed = fixed.ptr;
-        f.fixed_count = counters.ptr + 1;
-        f.cap = fixed.count;
-        f.error = flags.ptr + 1;
-        if ((e = cudaMemsetAsync(counters.ptr + 1, 0, 8, stream)) != cudaSuccess ||
-            (e = launch_fixup(rare.ptr, (int32_t)nrare, q.seed, f, stream)) != cudaSuccess ||
-            (e = cudaMemcpyAsync(pinned, counters.ptr + 1, 8, cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
-            (e = cudaMemcpyAsync((char*)pinned + 8, flags.ptr, 8, cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
+        if ((e = cudaMemcpyAsync(pinned, flags.ptr, 4, cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
+            (e = cudaMemcpyAsync((char*)pinned + 64, dhist, 2 * kHistBins * sizeof(unsigned int), cudaMemcpyDeviceToHost,
+                                 stream)) != cudaSuccess ||
             (e = cudaStreamSynchronize(stream)) != cudaSuccess) {
-            set_error("fixup", e);
+            set_error("flags", e);
             return false;
         }
-        ++last_launches;
-        const uint64_t nf = *(unsigned long long*)pinned;
-        const uint32_t* fl = (const uint32_t*)((char*)pinned + 8);
-        if (nf > fixed.count || fl[1]) { set_error("fixup overflow", cudaErrorUnknown); return false; }
-        if (nf) {
-            const size_t old = best.size();
-            best.resize(old + nf);
-            if ((e = cudaMemcpyAsync(best.data() + old, fixed.ptr, nf * sizeof(Hit), cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
-                (e = cudaStreamSynchronize(stream)) != cudaSuccess) {
-                set_error("copy", e);
-                return false;
-            }
-            for (size_t i = old; i < best.size(); ++i) ++h[best[i].count];
+        if (*(uint32_t*)pinned & 4u) { set_error("band engine: row-term copy timed out", cudaErrorLaunchTimeout); return false; }
+        if ((*(uint32_t*)pinned & 1u) && !exact) {
+            // A 4-row strip too dense for the byte-lane box: redo the search with the general scan.
+            band_fallbacks++;
+            std::fill(h.begin(), h.end(), 0u);
+            best.clear();
+            return scan_general(q, best, h, cancelled);
         }
+        const uint32_t* hs = (const uint32_t*)((const char*)pinned + 64);
+        const int32_t* hd = (const int32_t*)(hs + kHistBins);
+        for (int i = 0; i < kHistBins; ++i) h[i] = (uint32_t)((int64_t)hs[i] + hd[i]);
+        uint64_t total = 0, have = 0;
+        for (int c = q.min_size; c <= q.max_size; ++c) {
+            total += h[c];
+            if (c >= emit_min) have += h[c];
+        }
+        const uint64_t need = std::min<uint64_t>(total, (uint64_t)q.max_results);
+        if (have >= need || emit_min <= q.min_size) return true;
+        // Too few sites sent: the exact gate (highest count whose cumulative number covers need).
+        uint64_t acc = 0;
+        int32_t gate = q.max_size;
+        for (int c = q.max_size; c >= q.min_size; --c) {
+            acc += h[c];
+            gate = c;
+            if (acc >= need) break;
+        }
+        emit_min = gate;
     }
-    if ((e = cudaMemcpyAsync(pinned, flags.ptr, 4, cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
-        (e = cudaStreamSynchronize(stream)) != cudaSuccess) {
-        set_error("flags", e);
-        return false;
-    }
-    if (*(uint32_t*)pinned & 4u) { set_error("band engine: row-term copy timed out", cudaErrorLaunchTimeout); return false; }
-    if (*(uint32_t*)pinned && !exact) {
-        // A 4-row strip too dense for the byte-lane box: redo the search with the general scan.
-        band_fallbacks++;
-        std::fill(h.begin(), h.end(), 0u);
-        best.clear();
-        return scan_general(q, best, h, cancelled);
-    }
-    return true;
+    set_error("band gate did not converge", cudaErrorUnknown);
+    return false;
 }
 
 }  // namespace slime

@@ -274,7 +274,7 @@ int32_t Context::search_batch(const SearchSpec* reqs, int32_t n, ExtChunkResult*
             if (flags_h[4 * s] & 4u) { set_error("band engine: row-term copy timed out", cudaErrorLaunchTimeout); return -1; }
             if (emitted[s] && nrare && emitted[s] <= plan[s].hit_cap) {
                 if ((e = launch_filter_hits(bt_hits.ptr + plan[s].hit_off, (int64_t)emitted[s], bt_rare.ptr + plan[s].rare_off,
-                                            (int32_t)nrare, stream)) != cudaSuccess) {
+                                            (int32_t)nrare, false, stream)) != cudaSuccess) {
                     set_error("batch filter", e);
                     return -1;
                 }

@@ -90,6 +90,8 @@ struct BandArgs {
     int32_t indep;           // 1: independent bands (no shared LCG work, one X phase)
     int32_t exact;           // 1: bit-sliced exact counts of every centre (no bounds)
     uint32_t poll_limit;     // polls of a row-term mbarrier before the CTA gives up (bit 4 of overflow)
+    unsigned int* hist;      // if set: kHistBins counters of every centre in range, by count
+    int32_t emit_min;        // centres in range are appended to `out` only from this count on
     int64_t row_stride;      // input rows between band j and band j + 1 (2^17 with the shared LCG)
 };
 
@@ -132,6 +134,9 @@ struct FixArgs {
     unsigned long long* fixed_count;
     uint64_t cap;
     unsigned int* error;
+    // If set: per count, the change the fix-up makes to a scan histogram of first-draw counts
+    // (-1 at a fixed centre's first-draw count, +1 at its exact count, each when in range).
+    int* hist_delta;
 };
 
 void rare_target_table(std::vector<uint64_t>& targets, std::vector<uint32_t>& offsets);
@@ -140,7 +145,9 @@ cudaError_t launch_rare_scan(const uint64_t* targets, const uint32_t* offsets, i
                              uint32_t cap, unsigned int* count, cudaStream_t s);
 cudaError_t launch_fixup(const int2* rare, int32_t nrare, int64_t seed, const FixArgs& f,
                          cudaStream_t s);
-cudaError_t launch_filter_hits(Hit* hits, int64_t n, const int2* rare, int32_t nrare,
+// Marks hits whose window holds a rare chunk (count -1). With `sorted_by_x` the rare list is in
+// ascending x and each hit binary-searches it; otherwise every hit scans the whole list.
+cudaError_t launch_filter_hits(Hit* hits, int64_t n, const int2* rare, int32_t nrare, bool sorted_by_x,
                                cudaStream_t s);
 
 }  // namespace slime

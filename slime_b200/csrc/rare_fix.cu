@@ -65,13 +65,14 @@ __global__ void rare_scan_kernel(const uint64_t* targets, const uint32_t* offset
 __global__ void __launch_bounds__(256) fixup_kernel(const int2* rare, int32_t nrare, int64_t seed,
                                                     FixArgs f) {
     __shared__ uint64_t ex_rows[33];
+    __shared__ uint64_t fd_rows[33];  // first-draw bitmap: what the band scan counted
     __shared__ int near_n;
     __shared__ int2 near[32];
     const int r = blockIdx.x;
     if (r >= nrare) return;
     const int2 rc = rare[r];
     const int tid = threadIdx.x;
-    if (tid < 33) ex_rows[tid] = 0;
+    if (tid < 33) ex_rows[tid] = fd_rows[tid] = 0;
     if (tid == 0) near_n = 0;
     __syncthreads();
     // Earlier rare chunks close enough to share centres: those centres belong to them.
@@ -85,8 +86,9 @@ __global__ void __launch_bounds__(256) fixup_kernel(const int2* rare, int32_t nr
     for (int e = tid; e < 33 * 33; e += blockDim.x) {
         const int i = e / 33, j = e % 33;  // i: x offset, j: z offset
         const int32_t x = rc.x - 16 + i, z = rc.y - 16 + j;
-        if (slime_from_terms(x_term(x), z_term(z) + (uint64_t)seed))
-            atomicOr((unsigned long long*)&ex_rows[j], 1ULL << i);
+        const uint64_t xt = x_term(x), zt = z_term(z) + (uint64_t)seed;
+        if (slime_from_terms(xt, zt)) atomicOr((unsigned long long*)&ex_rows[j], 1ULL << i);
+        if (f.hist_delta && band::first_draw_slime(xt, zt)) atomicOr((unsigned long long*)&fd_rows[j], 1ULL << i);
     }
     __syncthreads();
     if (near_n > 32) {
@@ -110,9 +112,15 @@ __global__ void __launch_bounds__(256) fixup_kernel(const int2* rare, int32_t nr
             const int64_t ddx = (int64_t)cx - f.center_x, ddz = (int64_t)cz - f.center_z;
             if (ddx * ddx + ddz * ddz < f.rd_min_sq) continue;
         }
-        int ex = 0;
-        for (int i = 0; i < 17; ++i)  // region row dz + 8 + i holds window row i
+        int ex = 0, fd = 0;
+        for (int i = 0; i < 17; ++i) {  // region row dz + 8 + i holds window row i
             ex += __popc((uint32_t)(ex_rows[dz + 8 + i] >> (dx + 8)) & window_row_mask(i));
+            fd += __popc((uint32_t)(fd_rows[dz + 8 + i] >> (dx + 8)) & window_row_mask(i));
+        }
+        if (f.hist_delta) {
+            if (fd >= f.min_size && fd <= f.max_size) atomicAdd(&f.hist_delta[fd], -1);
+            if (ex >= f.min_size && ex <= f.max_size) atomicAdd(&f.hist_delta[ex], 1);
+        }
         if (ex >= f.min_size && ex <= f.max_size) {
             const unsigned long long k = atomicAdd(f.fixed_count, 1ULL);
             if (k < f.cap) f.fixed[k] = Hit{ex, cx, cz};
@@ -121,10 +129,22 @@ __global__ void __launch_bounds__(256) fixup_kernel(const int2* rare, int32_t nr
 }
 
 // Marks main-scan hits whose window holds a rare chunk (their first-draw count may be short).
-__global__ void filter_hits_kernel(Hit* hits, int64_t n, const int2* rs, int32_t nrare) {
+// With the rare list sorted by x, only the entries with |x - hit x| <= 8 are tested (binary search
+// for the first one); otherwise all are.
+__global__ void filter_hits_kernel(Hit* hits, int64_t n, const int2* rs, int32_t nrare, int sorted) {
     for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x) {
         const Hit h = hits[i];
-        for (int k = 0; k < nrare; ++k) {
+        int first = 0, last = nrare;
+        if (sorted) {
+            int lo = 0, hi = nrare;  // first entry with x >= hit x - 8
+            while (lo < hi) {
+                const int mid = (lo + hi) >> 1;
+                if ((int64_t)rs[mid].x < (int64_t)h.cx - 8) lo = mid + 1; else hi = mid;
+            }
+            first = lo;
+        }
+        for (int k = first; k < last; ++k) {
+            if (sorted && (int64_t)rs[k].x > (int64_t)h.cx + 8) break;
             // 64-bit: centres and rare chunks can lie millions of chunks apart.
             const int64_t dx = (int64_t)h.cx - rs[k].x, dz = (int64_t)h.cz - rs[k].y;
             if (dx * dx + dz * dz <= 68) {
@@ -179,11 +199,11 @@ cudaError_t launch_fixup(const int2* rare, int32_t nrare, int64_t seed, const Fi
     return cudaGetLastError();
 }
 
-cudaError_t launch_filter_hits(Hit* hits, int64_t n, const int2* rare, int32_t nrare,
+cudaError_t launch_filter_hits(Hit* hits, int64_t n, const int2* rare, int32_t nrare, bool sorted_by_x,
                                cudaStream_t s) {
     if (n <= 0 || nrare <= 0) return cudaSuccess;
     const int grid = (int)std::min<int64_t>((n + 255) / 256, 148 * 8);
-    filter_hits_kernel<<<grid, 256, 0, s>>>(hits, n, rare, nrare);
+    filter_hits_kernel<<<grid, 256, 0, s>>>(hits, n, rare, nrare, sorted_by_x ? 1 : 0);
     return cudaGetLastError();
 }
 

@@ -77,6 +77,7 @@ struct __align__(16) BandSmem {
     long long next_tile;                      // batched kernel: tile taken from the queue
     int search;                               // batched kernel: its search
     int failed;  // a bounded wait gave up: the CTA stops
+    unsigned int hist[kHistBins];             // counts of this CTA's centres in range (if args.hist)
 };
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) {
@@ -108,21 +109,16 @@ __device__ __forceinline__ bool bar_wait(unsigned long long* bar, uint32_t parit
     return false;
 }
 
-// Two-input add and subtract on the multiply pipe: `one` is 1 at run time, so the compiler emits
-// IMAD (the integer ALU pipe is the scan's bottleneck; the multiply pipe has room).
-__device__ __forceinline__ uint32_t madd(uint32_t a, uint32_t b, uint32_t one) { return a * one + b; }
-__device__ __forceinline__ uint32_t msub(uint32_t a, uint32_t b, uint32_t one) { return b * (0u - one) + a; }
-
-// Per nibble: the number of set bits (0..4). Shifts as multiply-highs, adds as multiply-adds.
-__device__ __forceinline__ uint32_t nibble_counts(uint32_t r, uint32_t one) {
-    const uint32_t a = msub(r, __umulhi(r, 1u << 31) & 0x55555555u, one);
-    return madd(a & 0x33333333u, __umulhi(a, 1u << 30) & 0x33333333u, one);
+// Per nibble: the number of set bits (0..4); shifts as multiply-highs.
+__device__ __forceinline__ uint32_t nibble_counts(uint32_t r) {
+    const uint32_t a = r - (__umulhi(r, 1u << 31) & 0x55555555u);
+    return (a & 0x33333333u) + (__umulhi(a, 1u << 30) & 0x33333333u);
 }
 
 // Per byte: high bit set where v >= t (v, t < 256; borrow-free because v | 0x80 >= 128 >= t').
 // Bytes >= 128 always report (a superset is safe: flagged groups are re-tested).
-__device__ __forceinline__ uint32_t bytes_at_least(uint32_t v, uint32_t t4, uint32_t one) {
-    return (msub(v | 0x80808080u, t4, one) | v) & 0x80808080u;
+__device__ __forceinline__ uint32_t bytes_at_least(uint32_t v, uint32_t t4) {
+    return (((v | 0x80808080u) - t4) | v) & 0x80808080u;
 }
 
 struct Tile {
@@ -187,7 +183,7 @@ constexpr int kSubgroupThreshold = 52;  // at or below: also test the four 2x2 s
 // of one centre over shuffled slices. Centres in range are appended to the hit list.
 // Warp-uniform arguments; called by the whole warp.
 template <bool kMasked, bool kIndep>
-__device__ __forceinline__ void exact_group(const BandSmem& S, const BandArgs& a, const Tile& T, int combo,
+__device__ __forceinline__ void exact_group(BandSmem& S, const BandArgs& a, const Tile& T, int combo,
                                          uint32_t fx, int word, int g, int st, int lane, uint32_t umask) {
     const int ph = combo_phase<kIndep>(combo), m = combo_band<kIndep>(combo);
     const int c0 = word * 32 + 4 * g;       // first window column (tile-relative input col)
@@ -231,6 +227,9 @@ __device__ __forceinline__ void exact_group(const BandSmem& S, const BandArgs& a
                 keep = ddx * ddx + ddz * ddz >= a.rd_min_sq;
             }
         }
+        // Every centre in range is counted; only those at or above the emission gate are sent.
+        if (keep && a.hist) atomicAdd(&S.hist[count], 1u);
+        keep = keep && count >= a.emit_min;
     }
     const unsigned mk = __ballot_sync(kFull, keep);
     if (mk) {
@@ -317,7 +316,7 @@ __device__ __forceinline__ void second_test(BandSmem& S, const BandArgs& a, cons
     const int r0 = 4 * (st - 4);  // rows 0 and 1 of strip st - 4
     uint32_t w0 = combo_word<kIndep>(S, r0, combo, fx, lane), w1 = combo_word<kIndep>(S, r0 + 1, combo, fx, lane);
     if (kMasked) { w0 &= cm; w1 &= cm; }
-    const uint32_t top01 = nibble_counts(w0, 1u) + nibble_counts(w1, 1u);
+    const uint32_t top01 = nibble_counts(w0) + nibble_counts(w1);
     // Outer cells of group g: 4-column blocks g and g + 4 of those four rows (byte lanes as in
     // the boxes: even groups from even blocks, odd groups from odd blocks).
     const uint32_t E = (top01 & 0x0F0F0F0Fu) + (n23 & 0x0F0F0F0Fu);
@@ -325,7 +324,7 @@ __device__ __forceinline__ void second_test(BandSmem& S, const BandArgs& a, cons
     // Lane 31 reads its own words here; only its groups 0..3 (which use no neighbour) can flag.
     const uint32_t En = __shfl_down_sync(kFull, E, 1), On = __shfl_down_sync(kFull, O, 1);
     const uint32_t oe = E + __funnelshift_r(E, En, 16), oo = O + __funnelshift_r(O, On, 16);
-    const uint32_t f2 = (bytes_at_least(re - oe, thr4, 1u) | (bytes_at_least(ro - oo, thr4, 1u) >> 1)) & flag;
+    const uint32_t f2 = (bytes_at_least(re - oe, thr4) | (bytes_at_least(ro - oo, thr4) >> 1)) & flag;
     uint32_t gm = 0;  // bit 8j+7 -> group 2j, bit 8j+6 -> group 2j+1
     for (uint32_t f = f2; f; f &= f - 1) {
         const int bit = __ffs(f) - 1;
@@ -378,7 +377,7 @@ template <bool kMasked, bool kIndep, bool kCands>
 __device__ __forceinline__ void count_strip(BandSmem& S, const BandArgs& a, const Tile& T, Counter& C,
                                             int slot, int t, int st, int warp, int lane, uint32_t fx,
                                             uint32_t lastmask, uint32_t thr4, uint32_t umask, uint32_t& guard,
-                                            int& ncand, uint32_t one) {
+                                            int& ncand) {
     const int r0 = 4 * t;  // t is a compile-time constant after unrolling
     const int hs = st % 5;
     const uint32_t live = st >= 4 ? lastmask : 0u;  // boxes are complete from the fifth strip on
@@ -398,25 +397,25 @@ __device__ __forceinline__ void count_strip(BandSmem& S, const BandArgs& a, cons
         for (int q = 0; q < 4; ++q) {
             uint32_t w = S.ring[slot][r0 + q][m][lane] & sel[q];
             if (kMasked) w &= C.cm[k];
-            n[q] = nibble_counts(w, one);
+            n[q] = nibble_counts(w);
         }
-        const uint32_t n01 = madd(n[0], n[1], one), n23 = madd(n[2], n[3], one);
-        const uint32_t e = madd(n01 & 0x0F0F0F0Fu, n23 & 0x0F0F0F0Fu, one);
-        const uint32_t o = madd(__umulhi(n01, 1u << 28) & 0x0F0F0F0Fu, __umulhi(n23, 1u << 28) & 0x0F0F0F0Fu, one);
+        const uint32_t n01 = n[0] + n[1], n23 = n[2] + n[3];
+        const uint32_t e = (n01 & 0x0F0F0F0Fu) + (n23 & 0x0F0F0F0Fu);
+        const uint32_t o = ((n01 >> 4) & 0x0F0F0F0Fu) + ((n23 >> 4) & 0x0F0F0F0Fu);
         // Lane 31 gets its own words back: they feed only groups 4..7, which it never flags.
         const uint32_t en = __shfl_down_sync(kFull, e, 1), on = __shfl_down_sync(kFull, o, 1);
-        const uint32_t s = madd(e, o, one), sn = madd(en, on, one);
+        const uint32_t s = e + o, sn = en + on;
         const uint32_t s1 = __funnelshift_r(s, sn, 8);
         const uint32_t ge = s + s1 + __funnelshift_r(e, en, 16);
         const uint32_t go = o + s1 + __funnelshift_r(s, sn, 16);
-        guard |= madd(ge, 0x4C4C4C4Cu, one) | madd(go, 0x4C4C4C4Cu, one);
+        guard |= (ge + 0x4C4C4C4Cu) | (go + 0x4C4C4C4Cu);
         uint32_t* he = &S.hist_e[hs][combo][lane];
         uint32_t* ho = &S.hist_o[hs][combo][lane];
-        C.re[k] = madd(C.re[k], msub(ge, *he, one), one);
-        C.ro[k] = madd(C.ro[k], msub(go, *ho, one), one);
+        C.re[k] += ge - *he;
+        C.ro[k] += go - *ho;
         *he = ge;
         *ho = go;
-        const uint32_t te = bytes_at_least(C.re[k], thr4, one), to = bytes_at_least(C.ro[k], thr4, one);
+        const uint32_t te = bytes_at_least(C.re[k], thr4), to = bytes_at_least(C.ro[k], thr4);
         fl[k] = (te | (to >> 1)) & live;  // even groups at bits 8j+7, odd groups at 8j+6
         n23s[k] = n23;
         any |= fl[k];
@@ -586,7 +585,7 @@ __device__ __forceinline__ int bs_value(const uint32_t (&cnt)[8], int j) {
 // combos; centres in [min_size, max_size] (and outside the rd_min disc) are appended to the hit
 // list. Called by the whole warp; lane = word.
 template <bool kMasked, bool kIndep>
-__device__ __forceinline__ void exact_strip(const BandSmem& S, const BandArgs& a, const Tile& T, const Counter& C,
+__device__ __forceinline__ void exact_strip(BandSmem& S, const BandArgs& a, const Tile& T, const Counter& C,
                                             int st, int warp, int lane, uint32_t fx) {
     constexpr int kUsed = kIndep ? kMaxBands / kWarps : kSlots;
     const int r0 = 4 * (st - 4);
@@ -636,8 +635,10 @@ __device__ __forceinline__ void exact_strip(const BandSmem& S, const BandArgs& a
             uint32_t pass = rowok ? colok & bs_at_least(cnt, a.min_size) : 0u;
             if (a.max_size < 221) pass &= ~bs_at_least(cnt, a.max_size + 1);
             if (!__any_sync(kFull, pass != 0)) continue;
-            // Append this lane's passing centres (outside the rd_min disc).
+            // This lane's centres in range outside the rd_min disc: all counted, those at or above
+            // the emission gate appended.
             const int64_t cv = v + band_v;
+            const uint32_t gate = a.emit_min > a.min_size ? bs_at_least(cnt, a.emit_min) : ~0u;
             uint32_t keep = 0;
             for (uint32_t p = pass; p; p &= p - 1) {
                 const int j = __ffs(p) - 1;
@@ -648,7 +649,8 @@ __device__ __forceinline__ void exact_strip(const BandSmem& S, const BandArgs& a
                     const int64_t ddx = (int64_t)cx - a.center_x, ddz = (int64_t)cz - a.center_z;
                     if (ddx * ddx + ddz * ddz < a.rd_min_sq) continue;
                 }
-                keep |= 1u << j;
+                if (a.hist) atomicAdd(&S.hist[bs_value(cnt, j)], 1u);
+                keep |= (gate >> j & 1u) << j;
             }
             const int n = __popc(keep);
             int pos = n;
@@ -695,6 +697,7 @@ __device__ __forceinline__ void band_cta_init(BandSmem& S, int tid) {
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
     for (int i = tid; i < kRingSlots * kBatchRows * kPlanes * kWords; i += kTpb) (&S.ring[0][0][0][0])[i] = 0;
+    for (int i = tid; i < kHistBins; i += kTpb) S.hist[i] = 0;
     __syncthreads();
 }
 
@@ -899,10 +902,10 @@ __device__ __forceinline__ bool band_tile(BandSmem& S, const BandArgs& a, int64_
             for (int t = 0; t < 2; ++t) {
                 if (interior)
                     count_strip<false, kIndep, kCands>(S, a, T, C, slot, t, 2 * b + t, warp, lane, fx, lastmask, thr4, umask,
-                                                       guard, ncand, one);
+                                                       guard, ncand);
                 else
                     count_strip<true, kIndep, kCands>(S, a, T, C, slot, t, 2 * b + t, warp, lane, fx, lastmask, thr4, umask,
-                                                      guard, ncand, one);
+                                                      guard, ncand);
             }
             // Candidates of this batch need rows of batches b-2..b, which stay in the ring until
             // batch b+2 is generated (after the next barrier).
@@ -933,6 +936,11 @@ __global__ void __launch_bounds__(kTpb, 1) band_scan_kernel(const BandArgs a) {
     band_cta_init(S, tid);
     for (int64_t tile = a.tile_begin + blockIdx.x; tile < a.tile_end; tile += gridDim.x)
         if (!band_tile<kMadAdd, kIndep, kCands, kExact>(S, a, tile, tid, lane, warp, bar_phase)) return;
+    if (a.hist) {
+        __syncthreads();
+        for (int i = tid; i < kHistBins; i += kTpb)
+            if (S.hist[i]) atomicAdd(&a.hist[i], S.hist[i]);
+    }
 }
 
 // Many searches in one persistent launch (each search independent-band or shared-LCG): each CTA

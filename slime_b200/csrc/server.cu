@@ -180,7 +180,7 @@ bool Server::finish_band(Job* j) {
     const uint64_t n = cnt[0];
     const uint32_t nrare = fl[2];
     std::vector<Hit> hits_h(n);
-    if (n && nrare && (e = launch_filter_hits(j->hits, (int64_t)n, j->rare, (int32_t)nrare, c.stream)) != cudaSuccess) {
+    if (n && nrare && (e = launch_filter_hits(j->hits, (int64_t)n, j->rare, (int32_t)nrare, false, c.stream)) != cudaSuccess) {
         c.set_error("server filter", e);
         return false;
     }

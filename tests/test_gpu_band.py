@@ -207,3 +207,22 @@ def test_bounded_wait_gives_up_cleanly(core, mode):
         core.lib.slime_b200_set_engine(0, 0)
     t_b, r_b = run(core, mode, *case)
     assert t_b == t_ok and np.array_equal(r_b, r_ok)
+
+
+@pytest.mark.parametrize("case", [
+    (777, 100_000, 40, 221, 0, 300_000, 300_000, 2000),       # ~6.8e6 sites: the emission gate is raised
+    (-888, 150_000, 41, 45, 60_000, 0, -1_500_000, 5000),    # gate with an upper bound and an annulus
+])
+def test_emission_gate_all_engines_agree_and_match_the_reference(core, case):
+    """Single band searches count every centre on the device and send only those at or above a
+    gate; totals come from the device histogram (corrected for rare chunks). All engines must give
+    the general scan's answer, and the reference GPU library's."""
+    t_g, r_g = run(core, 1, *case)
+    for mode in (3, 4, 5):
+        t_b, r_b = run(core, mode, *case)
+        assert t_b == t_g, mode
+        assert np.array_equal(r_b, r_g), mode
+    from tests.refcheck import ref_gpu
+    seed, r, lo, hi, rdm, cx, cz, maxr = case
+    t_r, r_r = ref_gpu().search(seed, r, lo, hi, rdm, cx, cz, maxr)
+    assert t_g == t_r and np.array_equal(r_g, r_r)
