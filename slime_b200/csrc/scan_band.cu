@@ -56,8 +56,10 @@ constexpr int row_words() { return kIndep ? kRowWordsI : kRowWords; }
 constexpr int kBatchRows = 8;               // rows per barrier: two 4-row strips
 // Generator layout: each lane evaluates bit `lane` of kGenW consecutive words (kGenW x 32 columns
 // per warp); kGenColWarps warps span the 32 words and each generates kGenRows rows of a batch.
+// Eight words per lane measured 4% faster on the full-world scan than four (fewer per-row setup
+// instructions per generated word), with identical output.
 #ifndef SLIME_GEN_WORDS
-#define SLIME_GEN_WORDS 4
+#define SLIME_GEN_WORDS 8
 #endif
 constexpr int kGenW = SLIME_GEN_WORDS;
 constexpr int kGenColWarps = 32 / kGenW;
@@ -564,6 +566,72 @@ __device__ __forceinline__ void bs_window_counts(const uint32_t (&Rr)[20], uint3
     bs_add<8, 5, 8>(d, a9, cnt);    // 221
 }
 
+// Number of set bits among 17 single-bit vectors (per bit position), as 5 planes: a carry-save
+// tree of 12 full adders and 3 half adders.
+__device__ __forceinline__ void bs_popcount17(const uint32_t (&b)[17], uint32_t (&o)[5]) {
+    uint32_t s1[5], c2[8];
+#pragma unroll
+    for (int i = 0; i < 5; ++i) bs_fa(b[3 * i], b[3 * i + 1], b[3 * i + 2], s1[i], c2[i]);
+    // weight 1: s1[0..4], b[15], b[16]
+    uint32_t t0, t1, u0;
+    bs_fa(s1[0], s1[1], s1[2], t0, c2[5]);
+    bs_fa(s1[3], s1[4], b[15], t1, c2[6]);
+    bs_fa(t0, t1, b[16], o[0], c2[7]);
+    // weight 2: c2[0..7]
+    uint32_t w2a, w2b, w4[4];
+    bs_fa(c2[0], c2[1], c2[2], w2a, w4[0]);
+    bs_fa(c2[3], c2[4], c2[5], w2b, w4[1]);
+    bs_fa(c2[6], c2[7], w2a, u0, w4[2]);
+    o[1] = u0 ^ w2b;
+    w4[3] = u0 & w2b;
+    // weight 4: w4[0..3]
+    uint32_t w4a, w8[2];
+    bs_fa(w4[0], w4[1], w4[2], w4a, w8[0]);
+    o[2] = w4a ^ w4[3];
+    w8[1] = w4a & w4[3];
+    o[3] = w8[0] ^ w8[1];
+    o[4] = w8[0] & w8[1];
+}
+
+// Window-relative vertical half-extent of column offset dx (0..16 from the window's first column):
+// the column holds window rows 8 - H .. 8 + H.
+__host__ __device__ constexpr int column_half_height(int dx) {
+    return dx == 0 || dx == 16 ? 2 : dx == 1 || dx == 15 ? 4 : dx == 2 || dx == 14 ? 5
+         : dx == 3 || dx == 13 ? 6 : dx <= 5 || dx >= 11 ? 7 : 8;
+}
+
+// Counts of the windows starting one row lower than `cnt` (window start DZ - 1 -> DZ among the
+// rows R / next-word rows Rn): per column one cell enters (row DZ + 8 + H) and one leaves (row
+// DZ + 7 - H), so count' = count + entering - leaving (mod 256, exact since counts are 0..221).
+template <int DZ>
+__device__ __forceinline__ void bs_slide(const uint32_t (&R)[20], const uint32_t (&Rn)[20], uint32_t (&cnt)[8]) {
+    uint32_t in[17], out[17];
+#pragma unroll
+    for (int dx = 0; dx < 17; ++dx) {
+        const int h = column_half_height(dx);
+        in[dx] = __funnelshift_r(R[DZ + 8 + h], Rn[DZ + 8 + h], dx);
+        out[dx] = __funnelshift_r(R[DZ + 7 - h], Rn[DZ + 7 - h], dx);
+    }
+    uint32_t a[5], b[5];
+    bs_popcount17(in, a);
+    bs_popcount17(out, b);
+    // count + a + ~b + 1 over 8 planes: carry-save, then a ripple add with carry-in 1.
+    uint32_t sv[8], cv[8];
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const uint32_t y = i < 5 ? a[i] : 0u, z = i < 5 ? ~b[i] : ~0u;
+        bs_fa(cnt[i], y, z, sv[i], cv[i]);
+    }
+    uint32_t c = ~0u;  // the +1 of the two's complement
+#pragma unroll
+    for (int i = 0; i < 8; ++i) {
+        const uint32_t y = i == 0 ? 0u : cv[i - 1];
+        uint32_t o;
+        bs_fa(sv[i], y, c, o, c);
+        cnt[i] = o;
+    }
+}
+
 // Centres whose count is at least t (t in 0..256): the carry out of count + (256 - t), with
 // the constant's bits known (one LOP3 per plane).
 __device__ __forceinline__ uint32_t bs_at_least(const uint32_t (&cnt)[8], int t) {
@@ -611,6 +679,12 @@ __device__ __forceinline__ void exact_strip(BandSmem& S, const BandArgs& a, cons
             colok = nv >= 32 ? ~0u : nv <= 0 ? 0u : (1u << nv) - 1u;
         }
         const int64_t band_v = (int64_t)(a.j0 + m) * a.row_stride;
+        // The next word's rows (lane 31 gets its own back: only its centres 16+, which lie beyond
+        // the tile's output columns, would read them).
+        uint32_t Rn[20];
+#pragma unroll
+        for (int i = 0; i < 20; ++i) Rn[i] = __shfl_down_sync(kFull, R[i], 1);
+        uint32_t cnt[8];
         // Annulus searches: skip the strip when all of its centres lie inside the rd_min disc
         // (warp-uniform: the strip's 4 rows across the tile's output columns).
         if (a.rd_min_sq) {
@@ -627,11 +701,11 @@ __device__ __forceinline__ void exact_strip(BandSmem& S, const BandArgs& a, cons
             const int rr = r0 + dz;  // window start row = centre row index in the tile
             const int64_t v = (int64_t)T.v0 + rr;
             const bool rowok = rr < T.out_h && v + band_v < a.height_v;
-            uint32_t cnt[8];
+            // The strip's first window row is counted in full; the next three slide down a row.
             if (dz == 0) bs_window_counts<0>(R, cnt);
-            else if (dz == 1) bs_window_counts<1>(R, cnt);
-            else if (dz == 2) bs_window_counts<2>(R, cnt);
-            else bs_window_counts<3>(R, cnt);
+            else if (dz == 1) bs_slide<1>(R, Rn, cnt);
+            else if (dz == 2) bs_slide<2>(R, Rn, cnt);
+            else bs_slide<3>(R, Rn, cnt);
             uint32_t pass = rowok ? colok & bs_at_least(cnt, a.min_size) : 0u;
             if (a.max_size < 221) pass &= ~bs_at_least(cnt, a.max_size + 1);
             if (!__any_sync(kFull, pass != 0)) continue;
@@ -897,15 +971,16 @@ __device__ __forceinline__ bool band_tile(BandSmem& S, const BandArgs& a, int64_
                     else exact_strip<true, kIndep>(S, a, T, C, 2 * b + t, warp, lane, fx);
                 }
                 continue;
-            }
+            } else {
 #pragma unroll
-            for (int t = 0; t < 2; ++t) {
-                if (interior)
-                    count_strip<false, kIndep, kCands>(S, a, T, C, slot, t, 2 * b + t, warp, lane, fx, lastmask, thr4, umask,
-                                                       guard, ncand);
-                else
-                    count_strip<true, kIndep, kCands>(S, a, T, C, slot, t, 2 * b + t, warp, lane, fx, lastmask, thr4, umask,
-                                                      guard, ncand);
+                for (int t = 0; t < 2; ++t) {
+                    if (interior)
+                        count_strip<false, kIndep, kCands>(S, a, T, C, slot, t, 2 * b + t, warp, lane, fx, lastmask, thr4,
+                                                           umask, guard, ncand);
+                    else
+                        count_strip<true, kIndep, kCands>(S, a, T, C, slot, t, 2 * b + t, warp, lane, fx, lastmask, thr4,
+                                                          umask, guard, ncand);
+                }
             }
             // Candidates of this batch need rows of batches b-2..b, which stay in the ring until
             // batch b+2 is generated (after the next barrier).
