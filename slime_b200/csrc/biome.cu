@@ -159,7 +159,9 @@ bool ensure_tables() {
     }
     for (int k = 0; k < BD_TREES; ++k) {
         const BdTree& b = BD_TREE[k];
-        if (b.depth > 8 || b.nparams > kParamSlots) {
+        // The tree search packs a node index (16 bits), a child count (8) and a depth (8) per
+        // stack level.
+        if (b.depth > 8 || b.nparams > kParamSlots || b.order > 255 || b.nnodes + b.steps[0] > 65535) {
             c.set_error_text("biome tables: tree shape out of range");
             return false;
         }

@@ -277,6 +277,22 @@ __device__ __forceinline__ int64_t axis_d2(int32_t v, int2 r) {
     return d * d;
 }
 
+// Distance of v to the range r along one axis. kWide: exact for every int32 v (64-bit
+// differences); otherwise 32-bit differences, exact while |v| <= 2^30 (range bounds are within
+// +-12,000, so no difference overflows).
+template <bool kWide>
+__device__ __forceinline__ uint32_t axis_gap(int32_t v, int2 r) {
+    if constexpr (kWide) {
+        return (uint32_t)(v > r.y ? (int64_t)v - r.y : v < r.x ? (int64_t)r.x - v : 0);
+    } else {
+        return (uint32_t)max(max(r.x - v, v - r.y), 0);
+    }
+}
+
+// The squared distance sum of one node's box plus g^2 (squares of 32-bit gaps, summed in 64 bits,
+// as the reference's int64 / uint64 arithmetic gives for these magnitudes).
+__device__ __forceinline__ uint64_t add_sq(uint64_t acc, uint32_t g) { return acc + (uint64_t)g * g; }
+
 // Nearest leaves of NQ queries that differ only in the depth axis (axis 4), in one traversal.
 // Each query follows exactly the reference's branch and bound (MinecraftGPUNoise.cu:686-809):
 // children of a node at tree depth d are `order` nodes steps[d] apart (a node whose subtree would
@@ -285,10 +301,10 @@ __device__ __forceinline__ int64_t axis_d2(int32_t v, int2 r) {
 // a bit mask keeps the queries that entered the subtree; the other queries neither descend nor
 // update there, so every query visits and decides exactly as a search of its own would.
 // Returns the biome ids (link byte of the best leaf) in biome[].
-template <int NQ>
-__device__ __forceinline__ void tree_nearest(const uint64_t* __restrict__ nodes, const int2* __restrict__ param,
-                                             const TreeGeom& g, const int32_t base[5], const int32_t (&depth)[NQ],
-                                             int32_t (&biome)[NQ]) {
+template <int NQ, bool kWide>
+__device__ __forceinline__ void tree_nearest_impl(const uint64_t* __restrict__ nodes, const int2* __restrict__ param,
+                                                  const TreeGeom& g, const int32_t base[5],
+                                                  const int32_t (&depth)[NQ], int32_t (&biome)[NQ]) {
     constexpr int kMaxDepth = 8;
     static_assert(NQ <= 32, "query mask is 32 bits");
     uint64_t ds[NQ];
@@ -298,43 +314,38 @@ __device__ __forceinline__ void tree_nearest(const uint64_t* __restrict__ nodes,
         ds[q] = ~0ull;
         best[q] = 0;
     }
-    int32_t st_child[kMaxDepth], st_left[kMaxDepth], st_depth[kMaxDepth];
-    uint32_t st_mask[kMaxDepth];
+    // Stack level: next child (bits 0-15), children left (16-23), tree depth (24-31); query mask.
+    uint32_t st_node[kMaxDepth], st_mask[kMaxDepth];
     int sp = 0;
     // Root: node 0 at depth 0, every query active.
     {
         int d = 0;
         while (d < g.depth && 0 + g.steps[d] >= g.nnodes) ++d;
-        st_child[0] = (int32_t)((nodes[0] >> 48) & 0xffff);
-        st_left[0] = g.order;
-        st_depth[0] = d;
+        st_node[0] = (uint32_t)((nodes[0] >> 48) & 0xffff) | ((uint32_t)g.order << 16) | ((uint32_t)d << 24);
         st_mask[0] = NQ == 32 ? 0xffffffffu : ((1u << NQ) - 1u);
     }
     while (sp >= 0) {
-        const int lvl = sp;
-        const int32_t child = st_child[lvl];
-        if (st_left[lvl] <= 0 || child >= g.nnodes) {
+        const uint32_t top = st_node[sp];
+        const int32_t child = (int32_t)(top & 0xffff);
+        const int left = (int)((top >> 16) & 0xff), d = (int)(top >> 24);
+        if (left <= 0 || child >= g.nnodes) {
             --sp;
             continue;
         }
-        const int d = st_depth[lvl];
-        st_child[lvl] = child + g.steps[d];
-        --st_left[lvl];
-        const uint32_t active = st_mask[lvl];
+        st_node[sp] = (uint32_t)(child + g.steps[d]) | ((uint32_t)(left - 1) << 16) | ((uint32_t)d << 24);
+        const uint32_t active = st_mask[sp];
         const uint64_t node = nodes[child];
         // The five depth-independent axes once, then the depth axis per query.
-        const int64_t b5 = axis_d2(base[0], param[node & 0xff]) + axis_d2(base[1], param[(node >> 8) & 0xff]) +
-                           axis_d2(base[2], param[(node >> 16) & 0xff]) +
-                           axis_d2(base[3], param[(node >> 24) & 0xff]) +
-                           axis_d2(base[4], param[(node >> 40) & 0xff]);
+        uint64_t b5 = add_sq(0, axis_gap<kWide>(base[0], param[node & 0xff]));
+        b5 = add_sq(b5, axis_gap<kWide>(base[1], param[(node >> 8) & 0xff]));
+        b5 = add_sq(b5, axis_gap<kWide>(base[2], param[(node >> 16) & 0xff]));
+        b5 = add_sq(b5, axis_gap<kWide>(base[3], param[(node >> 24) & 0xff]));
+        b5 = add_sq(b5, axis_gap<kWide>(base[4], param[(node >> 40) & 0xff]));
         const int2 rd = param[(node >> 32) & 0xff];
-        uint64_t dc[NQ];
         uint32_t enter = 0;
 #pragma unroll
-        for (int q = 0; q < NQ; ++q) {
-            dc[q] = (uint64_t)(b5 + axis_d2(depth[q], rd));
-            if (((active >> q) & 1u) && dc[q] < ds[q]) enter |= 1u << q;
-        }
+        for (int q = 0; q < NQ; ++q)
+            if (((active >> q) & 1u) && add_sq(b5, axis_gap<kWide>(depth[q], rd)) < ds[q]) enter |= 1u << q;
         if (!enter) continue;
         // The child sits at depth d + 1; a subtree that would run past the end descends in place.
         int cd = d + 1;
@@ -344,19 +355,35 @@ __device__ __forceinline__ void tree_nearest(const uint64_t* __restrict__ nodes,
 #pragma unroll
             for (int q = 0; q < NQ; ++q)
                 if ((enter >> q) & 1u) {
-                    ds[q] = dc[q];
+                    ds[q] = add_sq(b5, axis_gap<kWide>(depth[q], rd));
                     best[q] = child;
                 }
             continue;
         }
         ++sp;
-        st_child[sp] = (int32_t)((node >> 48) & 0xffff);
-        st_left[sp] = g.order;
-        st_depth[sp] = cd;
+        st_node[sp] = (uint32_t)((node >> 48) & 0xffff) | ((uint32_t)g.order << 16) | ((uint32_t)cd << 24);
         st_mask[sp] = enter;
     }
 #pragma unroll
     for (int q = 0; q < NQ; ++q) biome[q] = (int32_t)((nodes[best[q]] >> 48) & 0xff);
+}
+
+// The 32-bit-gap traversal when every coordinate is within +-2^30 (always, for climate values and
+// the depths of quart Y within the world), else the 64-bit one; both give the same leaves.
+template <int NQ>
+__device__ __forceinline__ void tree_nearest(const uint64_t* __restrict__ nodes, const int2* __restrict__ param,
+                                             const TreeGeom& g, const int32_t base[5], const int32_t (&depth)[NQ],
+                                             int32_t (&biome)[NQ]) {
+    constexpr int32_t kLim = 1 << 30;
+    bool wide = false;
+#pragma unroll
+    for (int i = 0; i < 5; ++i) wide |= base[i] > kLim || base[i] < -kLim;
+#pragma unroll
+    for (int q = 0; q < NQ; ++q) wide |= depth[q] > kLim || depth[q] < -kLim;
+    if (wide)
+        tree_nearest_impl<NQ, true>(nodes, param, g, base, depth, biome);
+    else
+        tree_nearest_impl<NQ, false>(nodes, param, g, base, depth, biome);
 }
 
 }  // namespace biome

@@ -127,15 +127,15 @@ struct Context {
     // autotune.py derived on B200 (slime_b200/tuning_b200.json).
     int32_t band_min_threshold = 46;
     int32_t band_min_periods = 9;
-    int32_t band_fast_threshold = 50;
+    int32_t band_fast_threshold = 48;
     int32_t band_fast_periods = 4;
     int32_t indep_min_threshold = 42;
-    int64_t indep_min_centres = 3600120001;
+    int64_t indep_min_centres = 400040001;
     // Below exact_below_threshold, areas of exact_min_centres centres or more use the band engines
     // with bit-sliced exact counts (shared LCG on areas band_fast_periods periods wide, else
     // independent bands), as long as the expected number of sites stays below kExactMaxSites.
-    int32_t exact_below_threshold = 46;
-    int64_t exact_min_centres = 100000000;
+    int32_t exact_below_threshold = 43;
+    int64_t exact_min_centres = 400040001;
     int64_t last_rare = 0;             // rare redraw chunks found by the last band search
     int64_t band_fallbacks = 0;        // band searches redone by the general scan
     int32_t band_mad_add = 1;          // generator variant: band adds on the multiply pipe

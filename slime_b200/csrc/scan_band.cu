@@ -914,6 +914,8 @@ __device__ __forceinline__ bool band_tile(BandSmem& S, const BandArgs& a, int64_
                 // Bands 0..count-1 of the row; returns count.
                 auto bands = [&](const int count) {
                     int m = 0;
+                    // Two band pairs per iteration (measured 2 % faster on the full-world scan).
+#pragma unroll 2
                     for (; m + 1 < count; m += 2) {
                         const uint2 z2 = *reinterpret_cast<const uint2*>(zr + m);  // m even: aligned
                         uint32_t wa[kGenW], wb[kGenW];

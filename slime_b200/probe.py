@@ -11,6 +11,8 @@ under a second):
   exact40     band_scan_kernel, independent bands with bit-sliced exact counts: radius 100,000,
               threshold 40
   band60      band_scan_kernel, shared LCG: radius 600,000 (9+ periods), threshold 60
+  world60     band_scan_kernel, shared LCG: the full-world threshold-60 scan (36 launches of ~60 ms,
+              under 1 GB on the device); profile one launch of it (`-c 1`)
   precise     precise_kernel: precise AFK scores of the best 20,000 sites of a threshold-36 search
   biome       biome chunk_kernel: the Deep Dark / Mushroom Fields filter of 4,096 threshold-48
               sites (version 26.2)
@@ -48,6 +50,13 @@ def run(case: str, repeat: int) -> dict:
             total, _ = core.search(SEED, 600_000, 60, 221, 0, 0, 0, 1000)
             out.update(total=int(total), kernel_ms=core.last_search_stats()[0],
                        T_centres_per_s=(2 * 600_000 + 1) ** 2 / core.last_search_stats()[0] / 1e9)
+        elif case == "world60":
+            from slime_b200 import workloads
+            spec = workloads.full_world_scan()
+            core.lib.slime_b200_set_engine(2, 0)
+            total, _ = core.search(spec.seed, spec.radius, 60, 221, 0, 0, 0, 1000)
+            out.update(total=int(total), kernel_ms=core.last_search_stats()[0],
+                       T_centres_per_s=(2 * spec.radius + 1) ** 2 / core.last_search_stats()[0] / 1e9)
         elif case == "precise":
             core.lib.slime_b200_set_engine(0, 0)
             _, sites = core.search(SEED, 20_000, 36, 221, 0, 0, 0, 20_000)
@@ -74,7 +83,7 @@ def run(case: str, repeat: int) -> dict:
 
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
-    ap.add_argument("case", choices=["general40", "exact40", "band60", "precise", "biome"])
+    ap.add_argument("case", choices=["general40", "exact40", "band60", "world60", "precise", "biome"])
     ap.add_argument("--repeat", type=int, default=2)
     a = ap.parse_args()
     print(json.dumps(run(a.case, a.repeat)))
