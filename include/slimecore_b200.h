@@ -118,26 +118,30 @@ void slime_b200_last_search_stats(double* kernel_ms, int64_t* launches);
  * that used the band engine; 0 otherwise. */
 int64_t slime_b200_last_rare_chunks(void);
 
-/* Engine selection: mode 0 automatic, 1 always the general scan, 2 the shared-LCG band engine
- * and 3 the independent-band engine whenever the threshold allows it (min_size >= 28), 4 / 5 the
- * shared-LCG / independent-band engine with bit-sliced exact counts (any threshold).
+/* Engine selection: mode 0 automatic, 1 always the general scan, 2 the shared-LCG band engine,
+ * 3 the independent-band engine and 6 the grouped-band engine whenever the threshold allows it
+ * (min_size >= 28), 4 / 5 the shared-LCG / independent-band engine with bit-sliced exact counts
+ * (any threshold).
  * `band_min_threshold` (28..221, other values keep the current one) is the smallest threshold
  * automatic mode sends to the shared-LCG band engine. Results are identical either way; only
  * speed differs. get_gpu_v1_algorithm() reports 100 (general), 200 (band), 300 (independent
- * bands), 210 or 310 (their exact-count modes) for the last search. */
+ * bands), 210 or 310 (their exact-count modes) or 220 (grouped bands) for the last search. */
 void slime_b200_set_engine(int32_t mode, int32_t band_min_threshold);
 
-/* The automatic engine rule as 6 or 8 numbers: {band_min_threshold, band_min_periods,
+/* The automatic engine rule as 6, 8 or 11 numbers: {band_min_threshold, band_min_periods,
  * band_fast_threshold, band_fast_periods, indep_min_threshold, indep_min_centres,
- * exact_below_threshold, exact_min_centres}. Thresholds below exact_below_threshold on areas of
+ * exact_below_threshold, exact_min_centres, grouped_min_threshold, grouped_min_width,
+ * grouped_max_width}. Thresholds below exact_below_threshold on areas of
  * exact_min_centres centres or more use the band engines with bit-sliced exact counts (shared LCG
  * on areas band_fast_periods x 2^17 chunks wide, else independent bands) while the expected
- * number of sites stays below 1e9. Otherwise the shared-LCG band engine takes areas at least
+ * number of sites stays below 1e9. Otherwise grouped bands (X phase pairs with groups of Z period
+ * copies) take areas grouped_min_width .. grouped_max_width chunks wide (at most 16 x 2^17) from
+ * grouped_min_threshold; the shared-LCG band engine takes areas at least
  * band_min_periods x 2^17 chunks wide from band_min_threshold, or band_fast_periods x 2^17 wide
- * from band_fast_threshold; independent bands take areas of indep_min_centres centres or more from
- * indep_min_threshold; the general scan takes the rest. Thresholds 28..222 (222 disables a branch;
- * exact_below_threshold 0..222, 0 disables it), periods 2..64. With n = 6 the exact-count numbers
- * are kept. Returns 0, or -1 for a wrong count or a value out of range (nothing is changed).
+ * from band_fast_threshold; independent bands take areas of indep_min_centres centres or more from indep_min_threshold; the
+ * general scan takes the rest. Thresholds 28..222 (222 disables a branch;
+ * exact_below_threshold 0..222, 0 disables it; grouped_min_threshold 28..222), periods 2..64,
+ * widths >= 0. With n = 6 or 8 the numbers not given are kept. Returns 0, or -1 for a wrong count or a value out of range (nothing is changed).
  * slime_b200/autotune.py measures the crossovers on the local GPU and writes them; the defaults are
  * B200 measurements. */
 int32_t slime_b200_set_engine_rule(const int64_t* rule, int32_t n);

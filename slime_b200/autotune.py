@@ -3,15 +3,18 @@
     python -m slime_b200.autotune [--out slime_b200/tuning_b200.json] [--quick]
 
 For each (radius, threshold) point of a grid the search is timed with every engine that applies
-(the general scan, independent bands, and the shared-LCG band engine where the area spans two
-periods, each of the band engines also with bit-sliced exact counts at low thresholds), forced
-through slime_b200_set_engine; every engine must return the same total and the same ranked sites.
-From the timings it derives the eight numbers of slime_b200_set_engine_rule:
+(the general scan, independent bands, grouped bands where the area spans a period, and the
+shared-LCG band engine where it spans two, the shared-LCG and independent-band engines also with
+bit-sliced exact counts at low thresholds), forced through slime_b200_set_engine; every engine
+must return the same total and the same ranked sites. From the timings it derives the eleven
+numbers of slime_b200_set_engine_rule:
 
   band_min_threshold, band_min_periods   shared LCG from this threshold on areas this many
   band_fast_threshold, band_fast_periods 2^17-chunk periods wide (two branches of the rule)
   indep_min_threshold, indep_min_centres independent bands instead of the general scan
   exact_below_threshold, exact_min_centres  exact counts below this threshold on areas this large
+  grouped_min_threshold, grouped_min_width, grouped_max_width
+                                         grouped bands from this threshold on areas this wide
 
 and writes them with the raw timings to a JSON file. SlimeCoreB200 applies that file when it
 loads the library. The general scan's rate does not depend on the area once it fills the GPU, so
@@ -44,11 +47,12 @@ def _time(core, mode, radius, thr, reps=2):
     return best, out
 
 
+GROUPED_MAX_PERIODS = 16  # grouped bands hold at most 16 period copies
 EXACT_MAX_THRESHOLD = 50  # the exact modes are timed up to here (their cost does not depend on it)
 
 
 def measure(core, quick=False):
-    radii = [10_000, 30_000, 100_000, 300_000, 600_000] + ([] if quick else [1_000_000])
+    radii = [10_000, 30_000, 100_000, 150_000, 200_000, 300_000, 600_000] + ([] if quick else [1_000_000])
     rows = []
     general_rate = {}
     for r in radii:
@@ -59,8 +63,10 @@ def measure(core, quick=False):
             engines = []
             if thr >= 42 or r <= 100_000:
                 engines += [("indep", 3)] + ([("band", 2)] if w >= 2 * PERIOD else [])
+                engines += [("grouped", 6)] if PERIOD < w <= GROUPED_MAX_PERIODS * PERIOD else []
             if thr <= EXACT_MAX_THRESHOLD:
                 engines += [("indep_exact", 5)] + ([("band_exact", 4)] if w >= 2 * PERIOD else [])
+                engines += [("grouped_exact", 7)] if PERIOD < w <= GROUPED_MAX_PERIODS * PERIOD else []
             if r <= 100_000:
                 engines.insert(0, ("general", 1))
             for name, mode in engines:
@@ -74,8 +80,9 @@ def measure(core, quick=False):
                 general_rate[thr] = point["centres"] / point["general_s"]
             else:
                 point["general_s"] = point["centres"] / general_rate.get(thr, min(general_rate.values()))
-            for k in ("indep", "band"):  # bounded engines below 42 on large areas: never chosen
-                if k + "_s" not in point and (k == "indep" or w >= 2 * PERIOD):
+            for k in ("indep", "band", "grouped"):  # bounded engines below 42 on large areas: never chosen
+                if k + "_s" not in point and (k == "indep" or (k == "band" and w >= 2 * PERIOD) or
+                                              (k == "grouped" and PERIOD < w <= GROUPED_MAX_PERIODS * PERIOD)):
                     point[k + "_s"] = float("inf")
             rows.append(point)
     core.lib.slime_b200_set_engine(0, 0)
@@ -83,10 +90,12 @@ def measure(core, quick=False):
 
 
 def derive(rows):
-    """The six rule numbers from the timings. Independent bands take a threshold when they beat
+    """The rule numbers from the timings. Independent bands take a threshold when they beat
     the general scan there and at every higher measured threshold of the area. The two
     shared-LCG branches are chosen among the measured (threshold, periods) crossovers as the pair
-    whose rule costs least over the whole grid (sum of each point's time over its best time)."""
+    whose rule costs least over the whole grid (sum of each point's time over its best time), and
+    the grouped-band branch (threshold, width range) is chosen the same way among the measured
+    thresholds and widths."""
     def min_winning_thr(pts, a, b):
         pts = sorted(pts, key=lambda p: p["threshold"])
         best = 222
@@ -107,14 +116,19 @@ def derive(rows):
     band_thr = {r: min_winning_thr(pts, "band_s", "indep_s") for r, pts in by_r.items()
                 if any("band_s" in p for p in pts)}
     cands = sorted({(t, (2 * r + 1) // PERIOD) for r, t in band_thr.items()} | {(222, 64)})
+    widths = sorted({2 * p["radius"] + 1 for p in rows if "grouped_s" in p})
+    g_cands = [(t, lo, hi) for t in sorted({p["threshold"] for p in rows} | {222})
+               for lo in widths for hi in widths if lo <= hi] or [(222, 1 << 40, 0)]
 
-    def cost(a, b):
+    def cost(a, b, g):
         total = 0.0
         for p in rows:
             w = 2 * p["radius"] + 1
-            best = min(p[k] for k in ("general_s", "indep_s", "band_s") if k in p)
+            best = min(p[k] for k in ("general_s", "indep_s", "band_s", "grouped_s") if k in p)
             thr = p["threshold"]
-            if "band_s" in p and any(thr >= t and w >= n * PERIOD for t, n in (a, b)):
+            if "grouped_s" in p and thr >= g[0] and g[1] <= w <= g[2]:
+                t_rule = p["grouped_s"]
+            elif "band_s" in p and any(thr >= t and w >= n * PERIOD for t, n in (a, b)):
                 t_rule = p["band_s"]
             elif w * w >= indep_min_centres and thr >= indep_min_threshold:
                 t_rule = p["indep_s"]
@@ -123,8 +137,14 @@ def derive(rows):
             total += t_rule / best
         return total
 
-    a, b = min(((x, y) for x in cands for y in cands), key=lambda ab: cost(*ab))
-    return [a[0], max(2, a[1]), b[0], max(2, b[1]), indep_min_threshold, indep_min_centres] + derive_exact(rows)
+    # Coordinate descent: the shared-LCG pair without grouped bands, the grouped triple given the
+    # pair, then the pair again given the triple.
+    g = (222, 1 << 40, 0)
+    a, b = min(((x, y) for x in cands for y in cands), key=lambda ab: cost(*ab, g))
+    g = min(g_cands, key=lambda gg: cost(a, b, gg))
+    a, b = min(((x, y) for x in cands for y in cands), key=lambda ab: cost(*ab, g))
+    return ([a[0], max(2, a[1]), b[0], max(2, b[1]), indep_min_threshold, indep_min_centres] + derive_exact(rows)
+            + [g[0], g[1], g[2]])
 
 
 def derive_exact(rows):
@@ -133,10 +153,10 @@ def derive_exact(rows):
     other engine on all areas of at least exact_min_centres centres, the smallest measured area
     where it wins at the lowest threshold."""
     def exact_best(p):
-        return min(p[k] for k in ("indep_exact_s", "band_exact_s") if k in p)
+        return min(p[k] for k in ("indep_exact_s", "band_exact_s", "grouped_exact_s") if k in p)
 
     def other_best(p):
-        return min(p[k] for k in ("general_s", "indep_s", "band_s") if k in p)
+        return min(p[k] for k in ("general_s", "indep_s", "band_s", "grouped_s") if k in p)
 
     pts = [p for p in rows if "indep_exact_s" in p]
     if not pts:
@@ -173,7 +193,8 @@ def main():
     doc = {"device": name.value.decode(errors="replace"),
            "rule": dict(zip(["band_min_threshold", "band_min_periods", "band_fast_threshold",
                              "band_fast_periods", "indep_min_threshold", "indep_min_centres",
-                             "exact_below_threshold", "exact_min_centres"], rule)),
+                             "exact_below_threshold", "exact_min_centres", "grouped_min_threshold",
+                             "grouped_min_width", "grouped_max_width"], rule)),
            "seed": SEED, "max_results": 200, "points": rows}
     Path(args.out).write_text(json.dumps(doc, indent=1) + "\n")
     print(json.dumps(doc["rule"]))

@@ -360,7 +360,7 @@ int64_t Context::search(const SearchSpec& q, ExtChunkResult* results) {
     last_rare = 0;
     const int32_t algo = engine_for(q);
     last_algorithm = algo;
-    last_shape = algo == kAlgoBand || algo == kAlgoBandExact ? 3
+    last_shape = algo == kAlgoBand || algo == kAlgoBandExact || algo == kAlgoGrouped || algo == kAlgoGroupedExact ? 3
                : algo == kAlgoIndep || algo == kAlgoIndepExact ? 4
                : (2 * q.rd_max + 1) < 8192 ? 1 : 2;
     // With a biome exclusion the scan keeps more ranked sites than max_results (some fail the
@@ -369,10 +369,9 @@ int64_t Context::search(const SearchSpec& q, ExtChunkResult* results) {
     if (q.biome_flags & 3)
         qs.max_results = (int32_t)std::min<int64_t>(INT32_MAX / 8, 2LL * q.max_results + 1024);
     for (;;) {
-        const bool indep = algo == kAlgoIndep || algo == kAlgoIndepExact;
-        const bool exact = algo == kAlgoBandExact || algo == kAlgoIndepExact;
+        const bool exact = algo_exact(algo);
         if (!(algo == kAlgoGeneral ? scan_general(qs, best, h, cancelled)
-                                   : scan_band(qs, best, h, cancelled, indep, exact))) {
+                                   : scan_band(qs, best, h, cancelled, band_mode_of(algo), exact))) {
             progress.store(0);
             return -1;
         }
@@ -641,18 +640,20 @@ int64_t slime_b200_set_wait_limit(int64_t polls) {
 
 void slime_b200_set_engine(int32_t mode, int32_t band_min_threshold) {
     std::lock_guard<std::mutex> lock(ctx().mu);
-    ctx().engine_override = (mode >= 0 && mode <= 5) ? mode : 0;
+    ctx().engine_override = (mode >= 0 && mode <= 7) ? mode : 0;
     if (band_min_threshold >= 28 && band_min_threshold <= 221) ctx().band_min_threshold = band_min_threshold;
 }
 
 const char* slime_b200_last_error(void) { return ctx().last_error; }
 
 int32_t slime_b200_set_engine_rule(const int64_t* rule, int32_t n) {
-    if (!rule || (n != 6 && n != 8)) return -1;
+    if (!rule || (n != 6 && n != 8 && n != 11)) return -1;
     const int64_t bt = rule[0], bp = rule[1], ft = rule[2], fp = rule[3], it = rule[4], ic = rule[5];
-    const int64_t et = n == 8 ? rule[6] : ctx().exact_below_threshold, ec = n == 8 ? rule[7] : ctx().exact_min_centres;
+    const int64_t et = n >= 8 ? rule[6] : ctx().exact_below_threshold, ec = n >= 8 ? rule[7] : ctx().exact_min_centres;
+    const int64_t gt = n == 11 ? rule[8] : ctx().grouped_min_threshold;
+    const int64_t gw = n == 11 ? rule[9] : ctx().grouped_min_width, gx = n == 11 ? rule[10] : ctx().grouped_max_width;
     if (bt < 28 || bt > 222 || ft < 28 || ft > 222 || it < 28 || it > 222 || bp < 2 || bp > 64 ||
-        fp < 2 || fp > 64 || ic < 0 || et < 0 || et > 222 || ec < 0)
+        fp < 2 || fp > 64 || ic < 0 || et < 0 || et > 222 || ec < 0 || gt < 28 || gt > 222 || gw < 0 || gx < 0)
         return -1;
     std::lock_guard<std::mutex> lock(ctx().mu);
     slime::Context& c = ctx();
@@ -664,11 +665,14 @@ int32_t slime_b200_set_engine_rule(const int64_t* rule, int32_t n) {
     c.indep_min_centres = ic;
     c.exact_below_threshold = (int32_t)et;
     c.exact_min_centres = ec;
+    c.grouped_min_threshold = (int32_t)gt;
+    c.grouped_min_width = gw;
+    c.grouped_max_width = gx;
     return 0;
 }
 
 int32_t slime_b200_get_engine_rule(int64_t* rule, int32_t n) {
-    if (!rule || (n != 6 && n != 8)) return -1;
+    if (!rule || (n != 6 && n != 8 && n != 11)) return -1;
     std::lock_guard<std::mutex> lock(ctx().mu);
     const slime::Context& c = ctx();
     rule[0] = c.band_min_threshold;
@@ -677,9 +681,14 @@ int32_t slime_b200_get_engine_rule(int64_t* rule, int32_t n) {
     rule[3] = c.band_fast_periods;
     rule[4] = c.indep_min_threshold;
     rule[5] = c.indep_min_centres;
-    if (n == 8) {
+    if (n >= 8) {
         rule[6] = c.exact_below_threshold;
         rule[7] = c.exact_min_centres;
+    }
+    if (n == 11) {
+        rule[8] = c.grouped_min_threshold;
+        rule[9] = c.grouped_min_width;
+        rule[10] = c.grouped_max_width;
     }
     return 0;
 }

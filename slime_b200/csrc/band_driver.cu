@@ -41,9 +41,11 @@ bool Context::ensure_band() {
 int32_t Context::engine_for(const SearchSpec& q) const {
     if (engine_override == 4) return kAlgoBandExact;
     if (engine_override == 5) return kAlgoIndepExact;
+    if (engine_override == 7) return kAlgoGroupedExact;
     if (engine_override == 1 || q.min_size < 28) return kAlgoGeneral;
     if (engine_override == 2) return kAlgoBand;
     if (engine_override == 3) return kAlgoIndep;
+    if (engine_override == 6) return kAlgoGrouped;
     // The rule's numbers are measured crossovers (slime_b200/autotune.py writes them; the
     // defaults are the B200 values). The shared LCG pays off with many periods (its work is
     // shared by every band and phase pair) and a high threshold.
@@ -53,7 +55,18 @@ int32_t Context::engine_for(const SearchSpec& q) const {
     constexpr double kExactMaxSites = 1e9;
     if (q.min_size < exact_below_threshold && w * w >= exact_min_centres &&
         (double)w * (double)w * tail_share(q.min_size) <= kExactMaxSites)
-        return w >= (int64_t)band_fast_periods * kP ? kAlgoBandExact : kAlgoIndepExact;
+        // Exact counts cost the same per centre in every mode; the generator's sharing decides:
+        // independent bands on narrow areas, grouped bands from 4 periods (measured on B200:
+        // 1.1-1.3 against 1.0 T/s at 4.6-9 periods, 0.9 against 1.0 at 3 periods), the shared
+        // LCG on the widest.
+        return w >= (int64_t)band_fast_periods * kP ? kAlgoBandExact
+               : w >= kGroupedExactMinPeriods * kP && w <= grouped_max_width && w <= kGroupedMaxPeriods * kP
+                   ? kAlgoGroupedExact
+                   : kAlgoIndepExact;
+    // Areas one to several periods wide: X phase pairs with groups of Z period copies.
+    if (q.min_size >= grouped_min_threshold && w >= grouped_min_width && w <= grouped_max_width &&
+        w <= kGroupedMaxPeriods * kP)
+        return kAlgoGrouped;
     if ((q.min_size >= band_min_threshold && w >= (int64_t)band_min_periods * kP) ||
         (q.min_size >= band_fast_threshold && w >= (int64_t)band_fast_periods * kP))
         return kAlgoBand;
@@ -61,19 +74,31 @@ int32_t Context::engine_for(const SearchSpec& q) const {
     return kAlgoGeneral;
 }
 
-BandGeom band_geometry(int64_t W, int64_t H, bool indep, int sm_count) {
+BandGeom band_geometry(int64_t W, int64_t H, int mode, int sm_count) {
     BandGeom g{};
+    const bool indep = mode == kBandIndep, grouped = mode == kBandGrouped;
     g.indep = indep;
-    g.transposed = !indep && W < 2 * kP && H >= 2 * kP;
+    g.transposed = mode == kBandShared && W < 2 * kP && H >= 2 * kP;
     g.width_u = g.transposed ? H : W;
     g.height_v = g.transposed ? W : H;
     const int out_w = band_tile_out_w();
     const int nb_max = band_max_bands();
     // Shared LCG: X phases and Z bands 2^17 apart. Independent bands: one phase, nJ bands of
-    // `stride` rows each (at least 256 rows a band, at most 32 bands).
+    // `stride` rows each (at least 256 rows a band, at most 32 bands). Grouped bands: X phase
+    // pairs and G groups of `copies` bands 2^17 apart (G a power of two, G * copies <= 16), group
+    // g starting at row g * stride with G * stride = 2^17 (or the whole height in one copy).
     g.nI = indep ? 1 : (g.width_u + kP - 1) / kP;
-    g.nJ = indep ? std::max<int64_t>(1, std::min<int64_t>(nb_max, g.height_v / 256)) : (g.height_v + kP - 1) / kP;
-    g.stride = indep ? (g.height_v + g.nJ - 1) / g.nJ : kP;
+    if (grouped) {
+        const int64_t copies = std::max<int64_t>(1, (g.height_v + kP - 1) / kP);
+        int64_t G = kGroupedMaxBands;
+        while (G > 1 && G * copies > kGroupedMaxBands) G >>= 1;
+        g.groups = (int32_t)G;
+        g.nJ = G * copies;
+        g.stride = copies > 1 ? kP / G : (g.height_v + G - 1) / G;
+    } else {
+        g.nJ = indep ? std::max<int64_t>(1, std::min<int64_t>(nb_max, g.height_v / 256)) : (g.height_v + kP - 1) / kP;
+        g.stride = indep ? (g.height_v + g.nJ - 1) / g.nJ : kP;
+    }
     g.ubase = (int32_t)(indep ? g.width_u : std::min(kP, g.width_u));
     g.vbase = (int32_t)std::min(g.stride, g.height_v);
     g.vrows = g.vbase + 16;
@@ -94,12 +119,13 @@ BandGeom band_geometry(int64_t W, int64_t H, bool indep, int sm_count) {
 }
 
 bool Context::scan_band(const SearchSpec& q, std::vector<Hit>& best, std::vector<uint32_t>& h,
-                        bool& cancelled, bool indep, bool exact) {
+                        bool& cancelled, int mode, bool exact) {
     if (!ensure_band()) return false;
     const int64_t W = 2 * q.rd_max + 1, H = W;
     const int32_t area_x0 = (int32_t)((int64_t)q.center_x - q.rd_max);
     const int32_t area_z0 = (int32_t)((int64_t)q.center_z - q.rd_max);
-    const BandGeom G = band_geometry(W, H, indep, sm_count);
+    const BandGeom G = band_geometry(W, H, mode, sm_count);
+    const bool indep = G.indep, split = G.indep || G.groups > 0;
     const bool transposed = G.transposed;
     const int64_t width_u = G.width_u, height_v = G.height_v;
     const int nb_max = band_max_bands();
@@ -108,7 +134,7 @@ bool Context::scan_band(const SearchSpec& q, std::vector<Hit>& best, std::vector
     const int64_t ngroups = G.ngroups;
     cudaError_t e;
     if ((e = xt.reserve((size_t)width_u + 16)) != cudaSuccess ||
-        (e = rt.reserve((size_t)ngroups * vrows_alloc * band_row_words(indep))) != cudaSuccess ||
+        (e = rt.reserve((size_t)ngroups * vrows_alloc * band_row_words(split))) != cudaSuccess ||
         (e = counters.reserve(4)) != cudaSuccess ||
         (e = hits.reserve(hit_capacity(q.max_results))) != cudaSuccess ||
         (e = fixed.reserve(1u << 20)) != cudaSuccess) {
@@ -118,7 +144,7 @@ bool Context::scan_band(const SearchSpec& q, std::vector<Hit>& best, std::vector
     const int32_t col_first = (transposed ? area_z0 : area_x0) - 8;
     const int32_t row_first = (transposed ? area_x0 : area_z0) - 8;
     if ((e = launch_band_terms(xt.ptr, col_first, (int32_t)(width_u + 16), rt.ptr, vrows_alloc, vrows,
-                               (int32_t)nJ, row_first, height_v + 16, stride, q.seed, transposed, indep,
+                               (int32_t)nJ, row_first, height_v + 16, stride, q.seed, transposed, indep, G.groups,
                                stream)) != cudaSuccess) {
         set_error("band terms", e);
         return false;
@@ -193,7 +219,7 @@ bool Context::scan_band(const SearchSpec& q, std::vector<Hit>& best, std::vector
                 BandArgs a{};
                 a.ct = xt.ptr;
                 a.ncols = width_u + 16;
-                a.rt = rt.ptr + (size_t)g * vrows_alloc * band_row_words(indep);
+                a.rt = rt.ptr + (size_t)g * vrows_alloc * band_row_words(split);
                 a.vrows = vrows;
                 a.vbase = vbase;
                 a.ubase = ubase;
@@ -221,6 +247,7 @@ bool Context::scan_band(const SearchSpec& q, std::vector<Hit>& best, std::vector
                 a.one = 1u;
                 a.mad_add = band_mad_add;
                 a.indep = indep ? 1 : 0;
+                a.groups = G.groups;
                 a.exact = exact ? 1 : 0;
                 a.poll_limit = wait_polls;
                 a.hist = dhist;

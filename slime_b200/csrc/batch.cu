@@ -50,6 +50,32 @@ constexpr uint64_t kHitCapMax = 16ull << 20;    // per search; larger searches r
 
 }  // namespace
 
+cudaError_t run_band_items(std::vector<BandArgs>& items, BandArgs* args_dev, int64_t* prefix_dev,
+                           unsigned long long* heads_dev, int grid, cudaStream_t s, int64_t* launches) {
+    const size_t m = items.size();
+    if (m == 0) return cudaSuccess;
+    std::stable_sort(items.begin(), items.end(),
+                     [](const BandArgs& x, const BandArgs& y) { return band_class(x) < band_class(y); });
+    std::vector<int64_t> prefix(m + 1, 0);
+    for (size_t i = 0; i < m; ++i) prefix[i + 1] = prefix[i] + (items[i].tile_end - items[i].tile_begin);
+    cudaError_t e;
+    if ((e = cudaMemcpyAsync(args_dev, items.data(), m * sizeof(BandArgs), cudaMemcpyHostToDevice, s)) != cudaSuccess ||
+        (e = cudaMemcpyAsync(prefix_dev, prefix.data(), (m + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, s)) != cudaSuccess ||
+        (e = cudaMemsetAsync(heads_dev, 0, kBandClasses * sizeof(unsigned long long), s)) != cudaSuccess)
+        return e;
+    for (size_t i0 = 0; i0 < m;) {
+        const int cls = band_class(items[i0]);
+        size_t i1 = i0 + 1;
+        while (i1 < m && band_class(items[i1]) == cls) ++i1;
+        if ((e = launch_band_batch(args_dev + i0, prefix_dev + i0, (int32_t)(i1 - i0), heads_dev + cls, cls, grid, s)) !=
+            cudaSuccess)
+            return e;
+        if (launches) ++*launches;
+        i0 = i1;
+    }
+    return cudaSuccess;
+}
+
 bool Context::collect_band(const SearchSpec& q, int32_t area_x0, int32_t area_z0, const Hit* hits_host,
                            uint64_t n, const int2* rare_dev, uint32_t nrare, unsigned long long* fixed_count_dev,
                            unsigned int* ferr_dev, std::vector<Hit>& best, std::vector<uint32_t>& h) {
@@ -130,7 +156,7 @@ int32_t Context::search_batch(const SearchSpec* reqs, int32_t n, ExtChunkResult*
         // The batch takes what the single search would run on a band engine (whatever the
         // area's size: small areas fill the GPU together); the general scan's searches run alone.
         const int32_t algo = engine_for(q);
-        const bool exact = algo == kAlgoBandExact || algo == kAlgoIndepExact;
+        const bool exact = algo_exact(algo);
         const bool band_ok = (q.min_size >= 28 || exact) && engine_override != 1 &&
                              (algo != kAlgoGeneral || q.min_size >= indep_min_threshold);
         if (!band_ok) {
@@ -141,7 +167,7 @@ int32_t Context::search_batch(const SearchSpec* reqs, int32_t n, ExtChunkResult*
         p.idx = i;
         p.exact = exact;
         const int64_t W = 2 * q.rd_max + 1;
-        p.g = band_geometry(W, W, algo != kAlgoBand && algo != kAlgoBandExact, sm_count);
+        p.g = band_geometry(W, W, algo == kAlgoGeneral ? kBandIndep : band_mode_of(algo), sm_count);
         p.area_x0 = (int32_t)((int64_t)q.center_x - q.rd_max);
         p.area_z0 = (int32_t)((int64_t)q.center_z - q.rd_max);
         const double centres = (double)W * (double)W;
@@ -158,7 +184,7 @@ int32_t Context::search_batch(const SearchSpec* reqs, int32_t n, ExtChunkResult*
         p.hit_off = hit_total;
         p.rare_off = rare_total;
         ct_total += (size_t)p.g.width_u + 16;
-        rt_total += (size_t)p.g.ngroups * p.g.vrows_alloc * band_row_words(p.g.indep);
+        rt_total += (size_t)p.g.ngroups * p.g.vrows_alloc * band_row_words(p.g.indep || p.g.groups > 0);
         hit_total += p.hit_cap;
         rare_total += p.rare_cap;
         plan.push_back(p);
@@ -166,7 +192,6 @@ int32_t Context::search_batch(const SearchSpec* reqs, int32_t n, ExtChunkResult*
     const int32_t m = (int32_t)plan.size();
 
     // ---- device work of the batched searches ------------------------------------------------
-    std::vector<int64_t> prefix((size_t)m + 1, 0);
     std::vector<uint64_t> emitted(m, 0), counts_h((size_t)m * 2, 0);
     std::vector<uint32_t> flags_h((size_t)m * 4, 0);
     std::vector<Hit> hits_h;
@@ -176,7 +201,7 @@ int32_t Context::search_batch(const SearchSpec* reqs, int32_t n, ExtChunkResult*
         // and fixed counters (u64).
         if ((e = bt_ct.reserve(ct_total)) != cudaSuccess || (e = bt_rt.reserve(rt_total)) != cudaSuccess ||
             (e = bt_hits.reserve(hit_total)) != cudaSuccess || (e = bt_rare.reserve(rare_total)) != cudaSuccess ||
-            (e = bt_flags.reserve((size_t)m * 4)) != cudaSuccess || (e = bt_counts.reserve((size_t)m * 2 + 1)) != cudaSuccess ||
+            (e = bt_flags.reserve((size_t)m * 4)) != cudaSuccess || (e = bt_counts.reserve((size_t)m * 2 + kBandClasses)) != cudaSuccess ||
             (e = bt_args.reserve((size_t)m)) != cudaSuccess || (e = bt_prefix.reserve((size_t)m + 1)) != cudaSuccess ||
             (e = fixed.reserve(1u << 20)) != cudaSuccess) {
             set_error("batch alloc", e);
@@ -220,13 +245,11 @@ int32_t Context::search_batch(const SearchSpec* reqs, int32_t n, ExtChunkResult*
             a.exact = p.exact ? 1 : 0;
             a.poll_limit = wait_polls;
             a.indep = g.indep ? 1 : 0;
+            a.groups = g.groups;
             a.row_stride = g.stride;
-            prefix[s + 1] = prefix[s] + g.tiles;
         }
         if ((e = cudaMemsetAsync(bt_flags.ptr, 0, (size_t)m * 4 * sizeof(unsigned int), stream)) != cudaSuccess ||
-            (e = cudaMemsetAsync(bt_counts.ptr, 0, ((size_t)m * 2 + 1) * sizeof(unsigned long long), stream)) != cudaSuccess ||
-            (e = cudaMemcpyAsync(bt_args.ptr, args.data(), (size_t)m * sizeof(BandArgs), cudaMemcpyHostToDevice, stream)) != cudaSuccess ||
-            (e = cudaMemcpyAsync(bt_prefix.ptr, prefix.data(), ((size_t)m + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, stream)) != cudaSuccess) {
+            (e = cudaMemsetAsync(bt_counts.ptr, 0, (size_t)m * 2 * sizeof(unsigned long long), stream)) != cudaSuccess) {
             set_error("batch setup", e);
             return -1;
         }
@@ -239,7 +262,7 @@ int32_t Context::search_batch(const SearchSpec* reqs, int32_t n, ExtChunkResult*
             const int32_t row_first = (g.transposed ? p.area_x0 : p.area_z0) - 8;
             if ((e = launch_band_terms(bt_ct.ptr + p.ct_off, col_first, (int32_t)(g.width_u + 16), bt_rt.ptr + p.rt_off,
                                        g.vrows_alloc, g.vrows, (int32_t)g.nJ, row_first, g.height_v + 16,
-                                       g.stride, q.seed, g.transposed, g.indep, stream)) != cudaSuccess ||
+                                       g.stride, q.seed, g.transposed, g.indep, g.groups, stream)) != cudaSuccess ||
                 (e = launch_rare_scan(rare_targets.ptr, rare_offsets.ptr, q.seed, p.area_z0 - 8, (int32_t)(W + 16),
                                       p.area_x0 - 8, (int32_t)(W + 16), bt_rare.ptr + p.rare_off, p.rare_cap,
                                       bt_flags.ptr + 4 * s + 2, stream)) != cudaSuccess) {
@@ -250,13 +273,12 @@ int32_t Context::search_batch(const SearchSpec* reqs, int32_t n, ExtChunkResult*
         }
         if (cancel.load()) { progress.store(0); return -1; }
         if ((e = cudaEventRecord(ev_a, stream)) != cudaSuccess ||
-            (e = launch_band_batch(bt_args.ptr, bt_prefix.ptr, m, bt_counts.ptr + 2 * m, band_mad_add != 0,
-                                   sm_count, stream)) != cudaSuccess ||
+            (e = run_band_items(args, bt_args.ptr, bt_prefix.ptr, bt_counts.ptr + 2 * m, sm_count, stream,
+                                &last_launches)) != cudaSuccess ||
             (e = cudaEventRecord(ev_b, stream)) != cudaSuccess) {
             set_error("batch scan", e);
             return -1;
         }
-        ++last_launches;
         // Rare-chunk counts, then the filter of each search's sites against its rare chunks.
         if ((e = cudaMemcpyAsync(flags_h.data(), bt_flags.ptr, (size_t)m * 4 * sizeof(unsigned int), cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
             (e = cudaMemcpyAsync(counts_h.data(), bt_counts.ptr, (size_t)m * 2 * sizeof(unsigned long long), cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||

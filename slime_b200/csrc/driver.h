@@ -61,6 +61,24 @@ constexpr int32_t kAlgoIndep = 300;
 // The band engines with bit-sliced exact counts of every centre (low thresholds).
 constexpr int32_t kAlgoBandExact = 210;
 constexpr int32_t kAlgoIndepExact = 310;
+// Grouped bands: X phase pairs and groups of Z period copies (areas one to a few periods wide).
+constexpr int32_t kAlgoGrouped = 220;
+constexpr int32_t kAlgoGroupedExact = 230;  // grouped bands with bit-sliced exact counts
+// Grouped bands hold at most this many bands; the rule uses them up to this width in periods.
+constexpr int64_t kGroupedMaxBands = 16;
+constexpr int64_t kGroupedMaxPeriods = 16;
+constexpr int64_t kGroupedExactMinPeriods = 4;  // exact counts: grouped bands from this width
+
+// Band mode (band_geometry) of a band algorithm.
+inline int band_mode_of(int32_t algo) {
+    return algo == kAlgoIndep || algo == kAlgoIndepExact                 ? kBandIndep
+           : algo == kAlgoGrouped || algo == kAlgoGroupedExact ? kBandGrouped
+                                                                : kBandShared;
+}
+// Band algorithms that count every centre exactly (bit-sliced).
+inline bool algo_exact(int32_t algo) {
+    return algo == kAlgoBandExact || algo == kAlgoIndepExact || algo == kAlgoGroupedExact;
+}
 
 constexpr size_t kPinnedBytes = 1 << 20;
 
@@ -118,17 +136,17 @@ struct Context {
     DeviceBuffer<int64_t> bt_prefix;
     bool band_ready = false;
     // 0 auto, 1 general scan, 2 band engine, 3 independent bands, 4 / 5 the band / independent-band
-    // engine with bit-sliced exact counts.
+    // engine with bit-sliced exact counts, 6 / 7 grouped bands (bounded / exact counts).
     int32_t engine_override = 0;
     // Engine rule (engine_for; slime_b200_set_engine_rule): the shared-LCG band engine for areas
     // at least band_min_periods periods wide from band_min_threshold, or band_fast_periods wide
     // from band_fast_threshold; independent bands for areas of indep_min_centres centres or more
     // from indep_min_threshold; the general scan otherwise. Defaults: the rule slime_b200/
     // autotune.py derived on B200 (slime_b200/tuning_b200.json).
-    int32_t band_min_threshold = 46;
-    int32_t band_min_periods = 9;
-    int32_t band_fast_threshold = 48;
-    int32_t band_fast_periods = 4;
+    int32_t band_min_threshold = 44;
+    int32_t band_min_periods = 15;
+    int32_t band_fast_threshold = 44;
+    int32_t band_fast_periods = 15;
     int32_t indep_min_threshold = 42;
     int64_t indep_min_centres = 400040001;
     // Below exact_below_threshold, areas of exact_min_centres centres or more use the band engines
@@ -136,6 +154,11 @@ struct Context {
     // independent bands), as long as the expected number of sites stays below kExactMaxSites.
     int32_t exact_below_threshold = 43;
     int64_t exact_min_centres = 400040001;
+    // Grouped bands for areas grouped_min_width .. grouped_max_width chunks wide (at most
+    // kGroupedMaxPeriods periods) from grouped_min_threshold, before the shared-LCG rule.
+    int32_t grouped_min_threshold = 46;
+    int64_t grouped_min_width = 200001;
+    int64_t grouped_max_width = 2000001;
     int64_t last_rare = 0;             // rare redraw chunks found by the last band search
     int64_t band_fallbacks = 0;        // band searches redone by the general scan
     int32_t band_mad_add = 1;          // generator variant: band adds on the multiply pipe
@@ -172,7 +195,7 @@ struct Context {
     bool ensure_band();
     int32_t engine_for(const SearchSpec& q) const;
     bool scan_band(const SearchSpec& q, std::vector<Hit>& best, std::vector<uint32_t>& hist_out,
-                   bool& cancelled, bool indep, bool exact = false);
+                   bool& cancelled, int mode, bool exact = false);
     bool score(int64_t seed, ExtChunkResult* host, int32_t n, int32_t scan_xz, bool pack);
     int64_t search(const SearchSpec& q, ExtChunkResult* results);
     // Total in range, ranked results and precise scores of a finished scan (-1 on failure). With

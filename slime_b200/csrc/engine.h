@@ -92,35 +92,50 @@ struct BandArgs {
     uint32_t poll_limit;     // polls of a row-term mbarrier before the CTA gives up (bit 4 of overflow)
     unsigned int* hist;      // if set: kHistBins counters of every centre in range, by count
     int32_t emit_min;        // centres in range are appended to `out` only from this count on
-    int64_t row_stride;      // input rows between band j and band j + 1 (2^17 with the shared LCG)
+    int64_t row_stride;      // input rows between band j and band j + 1 (2^17 with the shared LCG;
+                             // grouped bands: between group g and group g + 1)
+    int32_t groups;          // grouped bands (G > 0): band m = copy * G + group, copies 2^17 apart
+    int32_t pad_;
 };
 
 // Tiling of one band search (band_driver.cu): axes (u = phase axis, v = band axis), phases,
 // bands, base sizes and tiles, as the band kernels expect them.
 struct BandGeom {
     bool indep, transposed;
+    int32_t groups;  // grouped bands: G groups of nJ / G copies (0 otherwise)
     int64_t width_u, height_v, nI, nJ, stride, ngroups;
     int32_t ubase, vbase, vrows, vrows_alloc, band_h;
     int64_t u_tiles, v_tiles, pairs, tiles;
 };
-BandGeom band_geometry(int64_t W, int64_t H, bool indep, int sm_count);
+// Band modes of band_geometry.
+constexpr int kBandShared = 0, kBandIndep = 1, kBandGrouped = 2;
+BandGeom band_geometry(int64_t W, int64_t H, int mode, int sm_count);
 
 size_t band_smem_bytes();
 int band_tile_out_w();
 int band_max_bands();
 cudaError_t band_prepare();
 cudaError_t launch_band_scan(const BandArgs& a, int grid, cudaStream_t s);
-// Tiles of many band searches in one launch: args[i] (device) describes search i (either mode),
-// prefix[i] (device, nsearch + 1 entries) is its first tile in the batch, *head (device, zeroed)
-// is the tile queue. Item i runs tiles tile_begin .. tile_begin + prefix[i+1] - prefix[i] - 1 of
-// its search (tile_end is unused).
+// Tiles of many band searches of one launch class (band_class: band mode, survivor lists, exact
+// counts; kBandClasses of them) in one persistent launch: args[i] (device) describes search i,
+// prefix[i] (device, nsearch + 1 entries, increasing from any start) is its first tile in the
+// launch, *head (device, zeroed) is the tile queue. Item i runs tiles tile_begin .. tile_begin +
+// prefix[i+1] - prefix[i] - 1 of its search (tile_end is unused).
+constexpr int kBandClasses = 9;
+int band_class(const BandArgs& a);
 cudaError_t launch_band_batch(const BandArgs* args, const int64_t* prefix, int32_t nsearch,
-                              unsigned long long* head, bool mad_add, int grid, cudaStream_t s);
-int band_row_words(bool indep);
+                              unsigned long long* head, int cls, int grid, cudaStream_t s);
+// Uploads band work items of any classes (reordered by class in place) and runs them: one
+// persistent launch per class present. args_dev / prefix_dev hold items.size() (+1) entries,
+// heads_dev kBandClasses counters. Adds the launches made to *launches.
+cudaError_t run_band_items(std::vector<BandArgs>& items, BandArgs* args_dev, int64_t* prefix_dev,
+                           unsigned long long* heads_dev, int grid, cudaStream_t s, int64_t* launches);
+// Words of a row-term record: per-band low bits (independent and grouped bands) or shared ones.
+int band_row_words(bool split);
 cudaError_t launch_band_terms(uint64_t* ct, int32_t col_first, int32_t ncols, uint32_t* rt,
                               int32_t vrows_alloc, int32_t vrows, int32_t nj, int32_t row_first,
                               int64_t row_limit, int64_t row_stride, int64_t seed, bool transposed,
-                              bool indep, cudaStream_t s);
+                              bool indep, int32_t groups, cudaStream_t s);
 
 // ---- rare redraw correction (rare_fix.cu) ------------------------------------------------
 

@@ -34,6 +34,14 @@ constexpr int kWords = 32;                  // words per ring row: 1,024 base co
 constexpr int kOutW = kWords * 32 - 16;     // 1,008 centres per tile row
 constexpr int kMaxBands = 32;
 constexpr int kSwPlane = kMaxBands;         // plane of the phase-swap ballot
+// Band modes. Shared LCG: two X phases x up to 32 Z bands 2^17 apart, all sharing the low 17 bits
+// of the row term. Independent bands: one X phase x up to 32 bands at any row spacing. Grouped
+// bands: two X phases x up to 16 bands, in G groups at their own base rows, each group holding P
+// copies 2^17 apart that share its low bits (band m = copy * G + group); the swap ballot of group
+// g is plane kGrpSw + g.
+constexpr int kModeShared = 0, kModeIndep = 1, kModeGrouped = 2;
+constexpr int kGrpBands = 16;
+constexpr int kGrpSw = kGrpBands;
 constexpr int kPlanes = kMaxBands + 1;      // band planes and the swap plane
 constexpr int kMaxCombos = 2 * kMaxBands;
 constexpr int kSlots = kMaxCombos / kWarps; // combo rows counted per warp
@@ -50,8 +58,8 @@ constexpr int kRowValid = 33;   // bands of the group that hold this row (prefix
 constexpr int kRowWordsI = 72;
 constexpr int kRowLoI = 32;
 constexpr int kRowValidI = 64;
-template <bool kIndep>
-constexpr int row_words() { return kIndep ? kRowWordsI : kRowWords; }
+template <int kMode>
+constexpr int row_words() { return kMode == kModeShared ? kRowWords : kRowWordsI; }
 
 constexpr int kBatchRows = 8;               // rows per barrier: two 4-row strips
 // Generator layout: each lane evaluates bit `lane` of kGenW consecutive words (kGenW x 32 columns
@@ -79,6 +87,11 @@ struct __align__(16) BandSmem {
     long long next_tile;                      // batched kernel: tile taken from the queue
     int search;                               // batched kernel: its search
     int failed;  // a bounded wait gave up: the CTA stops
+    // Grouped bands, per band m: first area row (before the base row), swap plane, and all ones
+    // when its copy index is odd (the phase choice flips with each copy).
+    int32_t goff[kGrpBands];
+    int32_t gsw[kGrpBands];
+    uint32_t gflip[kGrpBands];
     unsigned int hist[kHistBins];             // counts of this CTA's centres in range (if args.hist)
 };
 
@@ -146,17 +159,25 @@ __device__ __forceinline__ uint32_t column_mask(const BandArgs& a, const Tile& T
 
 // A combo is one (X phase, band) pair: combo = 2 m + phase with the shared LCG, combo = m for
 // independent bands (one phase).
-template <bool kIndep>
-__device__ __forceinline__ int combo_band(int combo) { return kIndep ? combo : combo >> 1; }
-template <bool kIndep>
-__device__ __forceinline__ int combo_phase(int combo) { return kIndep ? 0 : combo & 1; }
+template <int kMode>
+__device__ __forceinline__ int combo_band(int combo) { return kMode == kModeIndep ? combo : combo >> 1; }
+template <int kMode>
+__device__ __forceinline__ int combo_phase(int combo) { return kMode == kModeIndep ? 0 : combo & 1; }
 
 // Bits of a combo in ring row `r` (tile-relative input row), word `word`.
-template <bool kIndep>
+template <int kMode>
 __device__ __forceinline__ uint32_t combo_word(const BandSmem& S, int r, int combo, uint32_t fx, int word) {
     const int slot = (r >> 3) & (kRingSlots - 1), q = r & 7;
-    if (kIndep) return S.ring[slot][q][combo][word];
-    return S.ring[slot][q][combo >> 1][word] & (S.ring[slot][q][kSwPlane][word] ^ fx);
+    if (kMode == kModeIndep) return S.ring[slot][q][combo][word];
+    const int m = combo >> 1;
+    if (kMode == kModeGrouped) return S.ring[slot][q][m][word] & (S.ring[slot][q][S.gsw[m]][word] ^ fx ^ S.gflip[m]);
+    return S.ring[slot][q][m][word] & (S.ring[slot][q][kSwPlane][word] ^ fx);
+}
+
+// First area row (band axis) of band m, before the tile's base row is added.
+template <int kMode>
+__device__ __forceinline__ int64_t band_row0(const BandSmem& S, const BandArgs& a, int m) {
+    return kMode == kModeGrouped ? (int64_t)S.goff[m] : (int64_t)(a.j0 + m) * a.row_stride;
 }
 
 // Row `r` (0..19) of the union of the 16 windows of a 4x4 centre group, as a 20-bit column mask:
@@ -184,16 +205,16 @@ constexpr int kSubgroupThreshold = 52;  // at or below: also test the four 2x2 s
 // reduction: below the threshold no window can reach it. Otherwise each lane counts half a window
 // of one centre over shuffled slices. Centres in range are appended to the hit list.
 // Warp-uniform arguments; called by the whole warp.
-template <bool kMasked, bool kIndep>
+template <bool kMasked, int kMode>
 __device__ __forceinline__ void exact_group(BandSmem& S, const BandArgs& a, const Tile& T, int combo,
                                          uint32_t fx, int word, int g, int st, int lane, uint32_t umask) {
-    const int ph = combo_phase<kIndep>(combo), m = combo_band<kIndep>(combo);
+    const int ph = combo_phase<kMode>(combo), m = combo_band<kMode>(combo);
     const int c0 = word * 32 + 4 * g;       // first window column (tile-relative input col)
     const int r0 = 4 * (st - 4);            // first window row (tile-relative input row)
     uint32_t slice = 0;
     if (lane < 20) {
-        uint32_t lo = combo_word<kIndep>(S, r0 + lane, combo, fx, word);
-        uint32_t hi = word + 1 < kWords ? combo_word<kIndep>(S, r0 + lane, combo, fx, word + 1) : 0u;
+        uint32_t lo = combo_word<kMode>(S, r0 + lane, combo, fx, word);
+        uint32_t hi = word + 1 < kWords ? combo_word<kMode>(S, r0 + lane, combo, fx, word + 1) : 0u;
         if (kMasked) {
             lo &= column_mask(a, T, word, ph);
             hi &= word + 1 < kWords ? column_mask(a, T, word + 1, ph) : 0u;
@@ -218,7 +239,7 @@ __device__ __forceinline__ void exact_group(BandSmem& S, const BandArgs& a, cons
         const int c = c0 + dx, rr = r0 + dz;
         const int64_t u = (int64_t)T.u0 + c, v = (int64_t)T.v0 + rr;
         const int64_t cu = u + (int64_t)(T.i0 + ph) * kPeriod;
-        const int64_t cv = v + (int64_t)(a.j0 + m) * a.row_stride;
+        const int64_t cv = v + band_row0<kMode>(S, a, m);
         keep = count >= a.min_size && count <= a.max_size && c < kOutW && u < a.ubase &&
                rr < T.out_h && cu < a.width_u && cv < a.height_v;
         if (keep) {
@@ -258,7 +279,7 @@ struct Counter {
 // borrows). Survivors are counted exactly. Called by the whole warp.
 // The union counts of the warp's candidate groups, 32 at a time (lane = group), then the exact
 // counts of those that reach the threshold. Called by the whole warp; the caller empties the list.
-template <bool kMasked, bool kIndep>
+template <bool kMasked, int kMode>
 __device__ __forceinline__ void flush_cands(BandSmem& S, const BandArgs& a, const Tile& T, uint32_t fx, int warp,
                                          int lane, uint32_t umask, int ncand) {
     __syncwarp();
@@ -272,16 +293,16 @@ __device__ __forceinline__ void flush_cands(BandSmem& S, const BandArgs& a, cons
             const int r0 = 4 * ((int)(e & 0xFFFF) - 4);
             uint32_t cml = ~0u, cmh = word + 1 < kWords ? ~0u : 0u;
             if (kMasked) {
-                cml = column_mask(a, T, word, combo_phase<kIndep>(combo));
-                cmh &= word + 1 < kWords ? column_mask(a, T, word + 1, combo_phase<kIndep>(combo)) : 0u;
+                cml = column_mask(a, T, word, combo_phase<kMode>(combo));
+                cmh &= word + 1 < kWords ? column_mask(a, T, word + 1, combo_phase<kMode>(combo)) : 0u;
             }
             const int wh = min(word + 1, kWords - 1);
             if (a.min_size > kSubgroupThreshold) {
                 int sum = 0;
 #pragma unroll
                 for (int r = 0; r < 20; ++r) {
-                    const uint32_t lo = combo_word<kIndep>(S, r0 + r, combo, fx, word) & cml;
-                    const uint32_t hi = combo_word<kIndep>(S, r0 + r, combo, fx, wh) & cmh;
+                    const uint32_t lo = combo_word<kMode>(S, r0 + r, combo, fx, word) & cml;
+                    const uint32_t hi = combo_word<kMode>(S, r0 + r, combo, fx, wh) & cmh;
                     sum += __popc(__funnelshift_r(lo, hi, 4 * g) & group_union_mask(r));
                 }
                 pass = sum >= a.min_size;
@@ -289,8 +310,8 @@ __device__ __forceinline__ void flush_cands(BandSmem& S, const BandArgs& a, cons
                 int sum = 0, s0 = 0, s1 = 0, s2 = 0, s3 = 0;
 #pragma unroll
                 for (int r = 0; r < 20; ++r) {
-                    const uint32_t lo = combo_word<kIndep>(S, r0 + r, combo, fx, word) & cml;
-                    const uint32_t hi = combo_word<kIndep>(S, r0 + r, combo, fx, wh) & cmh;
+                    const uint32_t lo = combo_word<kMode>(S, r0 + r, combo, fx, word) & cml;
+                    const uint32_t hi = combo_word<kMode>(S, r0 + r, combo, fx, wh) & cmh;
                     const uint32_t x = __funnelshift_r(lo, hi, 4 * g);
                     sum += __popc(x & group_union_mask(r));
                     s0 += __popc(x & subgroup_union_mask(r, 0, 0));
@@ -303,20 +324,20 @@ __device__ __forceinline__ void flush_cands(BandSmem& S, const BandArgs& a, cons
         }
         for (unsigned pm = __ballot_sync(kFull, pass); pm; pm &= pm - 1) {
             const uint32_t ee = __shfl_sync(kFull, e, __ffs(pm) - 1);
-            exact_group<kMasked, kIndep>(S, a, T, (int)(ee >> 24), fx, (int)((ee >> 19) & 31), (int)((ee >> 16) & 7),
+            exact_group<kMasked, kMode>(S, a, T, (int)(ee >> 24), fx, (int)((ee >> 19) & 31), (int)((ee >> 16) & 7),
                                          (int)(ee & 0xFFFF), lane, umask);
         }
     }
     __syncwarp();
 }
 
-template <bool kMasked, bool kIndep, bool kCands>
+template <bool kMasked, int kMode, bool kCands>
 __device__ __forceinline__ void second_test(BandSmem& S, const BandArgs& a, const Tile& T, uint32_t flag,
                                             uint32_t re, uint32_t ro, uint32_t n23, uint32_t cm, uint32_t fx,
                                             uint32_t thr4, int combo, int lane, int st, uint32_t umask, int warp,
                                             int& ncand) {
     const int r0 = 4 * (st - 4);  // rows 0 and 1 of strip st - 4
-    uint32_t w0 = combo_word<kIndep>(S, r0, combo, fx, lane), w1 = combo_word<kIndep>(S, r0 + 1, combo, fx, lane);
+    uint32_t w0 = combo_word<kMode>(S, r0, combo, fx, lane), w1 = combo_word<kMode>(S, r0 + 1, combo, fx, lane);
     if (kMasked) { w0 &= cm; w1 &= cm; }
     const uint32_t top01 = nibble_counts(w0) + nibble_counts(w1);
     // Outer cells of group g: 4-column blocks g and g + 4 of those four rows (byte lanes as in
@@ -336,7 +357,7 @@ __device__ __forceinline__ void second_test(BandSmem& S, const BandArgs& a, cons
         for (unsigned todo = __ballot_sync(kFull, gm != 0); todo; todo &= todo - 1) {
             const int word = __ffs(todo) - 1;
             for (uint32_t gw = __shfl_sync(kFull, gm, word); gw; gw &= gw - 1)
-                exact_group<kMasked, kIndep>(S, a, T, combo, fx, word, __ffs(gw) - 1, st, lane, umask);
+                exact_group<kMasked, kMode>(S, a, T, combo, fx, word, __ffs(gw) - 1, st, lane, umask);
         }
         return;
     }
@@ -364,7 +385,7 @@ __device__ __forceinline__ void second_test(BandSmem& S, const BandArgs& a, cons
         ncand += took;
         placed += took;
         if (placed == total) break;
-        flush_cands<kMasked, kIndep>(S, a, T, fx, warp, lane, umask, ncand);
+        flush_cands<kMasked, kMode>(S, a, T, fx, warp, lane, umask, ncand);
         ncand = 0;
     }
     __syncwarp();
@@ -375,7 +396,7 @@ __device__ __forceinline__ void second_test(BandSmem& S, const BandArgs& a, cons
 // threshold test. Only when a lane flags a group does the warp take the second test. With the
 // shared LCG, slots of combos beyond the launch's band count read zero planes and never flag;
 // independent bands use two slots per warp (32 combos) and skip combos beyond the band count.
-template <bool kMasked, bool kIndep, bool kCands>
+template <bool kMasked, int kMode, bool kCands>
 __device__ __forceinline__ void count_strip(BandSmem& S, const BandArgs& a, const Tile& T, Counter& C,
                                             int slot, int t, int st, int warp, int lane, uint32_t fx,
                                             uint32_t lastmask, uint32_t thr4, uint32_t umask, uint32_t& guard,
@@ -383,21 +404,25 @@ __device__ __forceinline__ void count_strip(BandSmem& S, const BandArgs& a, cons
     const int r0 = 4 * t;  // t is a compile-time constant after unrolling
     const int hs = st % 5;
     const uint32_t live = st >= 4 ? lastmask : 0u;  // boxes are complete from the fifth strip on
-    constexpr int kUsed = kIndep ? kMaxBands / kWarps : kSlots;
+    constexpr int kUsed = kMode == kModeShared ? kSlots : kMaxBands / kWarps;
     uint32_t sel[4];
 #pragma unroll
-    for (int q = 0; q < 4; ++q) sel[q] = kIndep ? ~0u : S.ring[slot][r0 + q][kSwPlane][lane] ^ fx;
+    for (int q = 0; q < 4; ++q) sel[q] = kMode == kModeShared ? S.ring[slot][r0 + q][kSwPlane][lane] ^ fx : ~0u;
     uint32_t fl[kSlots] = {}, n23s[kSlots] = {};
     uint32_t any = 0;
 #pragma unroll
     for (int k = 0; k < kUsed; ++k) {
         const int combo = warp + kWarps * k;
-        const int m = combo_band<kIndep>(combo);
-        if (kIndep && m >= a.nb) continue;  // warp-uniform
+        const int m = combo_band<kMode>(combo);
+        if (kMode != kModeShared && m >= a.nb) continue;  // warp-uniform
         uint32_t n[4];
+        // Grouped bands: the slot's own swap plane and phase sense.
+        const int gs = kMode == kModeGrouped ? S.gsw[m] : 0;
+        const uint32_t gfx = kMode == kModeGrouped ? fx ^ S.gflip[m] : 0u;
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
-            uint32_t w = S.ring[slot][r0 + q][m][lane] & sel[q];
+            uint32_t w = S.ring[slot][r0 + q][m][lane] &
+                         (kMode == kModeGrouped ? S.ring[slot][r0 + q][gs][lane] ^ gfx : sel[q]);
             if (kMasked) w &= C.cm[k];
             n[q] = nibble_counts(w);
         }
@@ -426,7 +451,7 @@ __device__ __forceinline__ void count_strip(BandSmem& S, const BandArgs& a, cons
 #pragma unroll
         for (int k = 0; k < kUsed; ++k)
             if (__any_sync(kFull, fl[k] != 0))
-                second_test<kMasked, kIndep, kCands>(S, a, T, fl[k], C.re[k], C.ro[k], n23s[k], kMasked ? C.cm[k] : ~0u,
+                second_test<kMasked, kMode, kCands>(S, a, T, fl[k], C.re[k], C.ro[k], n23s[k], kMasked ? C.cm[k] : ~0u,
                                              fx, thr4, warp + kWarps * k, lane, st, umask, warp, ncand);
     }
 }
@@ -652,22 +677,22 @@ __device__ __forceinline__ int bs_value(const uint32_t (&cnt)[8], int j) {
 // Exact counts of strip st (window rows 4(st-4) .. 4st+3, centres of 4 rows) for the warp's
 // combos; centres in [min_size, max_size] (and outside the rd_min disc) are appended to the hit
 // list. Called by the whole warp; lane = word.
-template <bool kMasked, bool kIndep>
+template <bool kMasked, int kMode>
 __device__ __forceinline__ void exact_strip(BandSmem& S, const BandArgs& a, const Tile& T, const Counter& C,
                                             int st, int warp, int lane, uint32_t fx) {
-    constexpr int kUsed = kIndep ? kMaxBands / kWarps : kSlots;
+    constexpr int kUsed = kMode == kModeShared ? kSlots : kMaxBands / kWarps;
     const int r0 = 4 * (st - 4);
     // Output columns of this word: centre index c = 32 lane + j < kOutW and inside the area.
     const int64_t u_first = (int64_t)T.u0 + 32 * lane;
 #pragma unroll 1
     for (int k = 0; k < kUsed; ++k) {
         const int combo = warp + kWarps * k;
-        const int m = combo_band<kIndep>(combo), ph = combo_phase<kIndep>(combo);
+        const int m = combo_band<kMode>(combo), ph = combo_phase<kMode>(combo);
         if (m >= a.nb) continue;  // warp-uniform: planes of bands beyond the count are empty
         uint32_t R[20];
 #pragma unroll
         for (int i = 0; i < 20; ++i) {
-            uint32_t w = combo_word<kIndep>(S, r0 + i, combo, fx, lane);
+            uint32_t w = combo_word<kMode>(S, r0 + i, combo, fx, lane);
             if (kMasked) w &= C.cm[k];
             R[i] = w;
         }
@@ -678,7 +703,7 @@ __device__ __forceinline__ void exact_strip(BandSmem& S, const BandArgs& a, cons
             const int64_t nv = min(ulim - u_first, (int64_t)kOutW - 32 * lane);
             colok = nv >= 32 ? ~0u : nv <= 0 ? 0u : (1u << nv) - 1u;
         }
-        const int64_t band_v = (int64_t)(a.j0 + m) * a.row_stride;
+        const int64_t band_v = band_row0<kMode>(S, a, m);
         // The next word's rows (lane 31 gets its own back: only its centres 16+, which lie beyond
         // the tile's output columns, would read them).
         uint32_t Rn[20];
@@ -777,7 +802,7 @@ __device__ __forceinline__ void band_cta_init(BandSmem& S, int tid) {
 
 // One tile of one search (block-uniform arguments; all threads). Returns false when a bounded
 // wait gave up (the search's overflow word gets bit 4 and the CTA must stop).
-template <bool kMadAdd, bool kIndep, bool kCands, bool kExact = false>
+template <bool kMadAdd, int kMode, bool kCands, bool kExact = false>
 __device__ __forceinline__ bool band_tile(BandSmem& S, const BandArgs& a, int64_t tile, int tid, int lane,
                                           int warp, uint32_t& bar_phase) {
     const int nb = a.nb;
@@ -785,7 +810,8 @@ __device__ __forceinline__ bool band_tile(BandSmem& S, const BandArgs& a, int64_
     const uint32_t one = a.one;  // 1 at run time: keeps the band add on the multiply pipe
     // Counter constants: the swap sense of the warp's phase and the groups lane 31 may flag
     // (groups 4..7 of word 31 hold centres 1,008+ of the tile, which belong to the next tile).
-    const uint32_t fx = ((warp ^ (warp >> 1)) & 1) ? 0u : ~0u;
+    // (Grouped bands: the phase alone; each band's copy parity is applied per combo.)
+    const uint32_t fx = kMode == kModeGrouped ? ((warp & 1) ? 0u : ~0u) : (((warp ^ (warp >> 1)) & 1) ? 0u : ~0u);
     const uint32_t lastmask = lane == kWords - 1 ? 0x0000C0C0u : ~0u;
     const uint32_t umask = lane < 20 ? group_union_mask(lane) : 0u;
     uint32_t guard = 0;
@@ -795,7 +821,7 @@ __device__ __forceinline__ bool band_tile(BandSmem& S, const BandArgs& a, int64_
         const int ut = (int)(tile % a.u_tiles);
         const int64_t rest = tile / a.u_tiles;
         const int vt = (int)(rest % a.v_tiles);
-        T.i0 = kIndep ? 0 : 2 * (int)(rest / a.v_tiles);
+        T.i0 = kMode == kModeIndep ? 0 : 2 * (int)(rest / a.v_tiles);
         T.u0 = ut * kOutW;
         T.v0 = vt * a.band_h;
         // Tiles with no centre of the area in any of their combos are skipped (block-uniform).
@@ -805,7 +831,7 @@ __device__ __forceinline__ bool band_tile(BandSmem& S, const BandArgs& a, int64_
         T.out_h = min(a.band_h, a.vbase - T.v0);
         const int strips = (T.out_h + 16 + 3) / 4;
         const int batches = (strips + 1) / 2;
-        constexpr int kRW = row_words<kIndep>();
+        constexpr int kRW = row_words<kMode>();
         constexpr uint32_t kBatchBytes = kBatchRows * kRW * 4;
 
         // Generator columns of this thread: words kGenW*(warp % kGenColWarps) .. + kGenW - 1, lane =
@@ -825,15 +851,22 @@ __device__ __forceinline__ bool band_tile(BandSmem& S, const BandArgs& a, int64_
         Counter C;
 #pragma unroll
         for (int k = 0; k < kSlots; ++k) {
-            C.cm[k] = column_mask(a, T, lane, combo_phase<kIndep>(warp + kWarps * k));
+            C.cm[k] = column_mask(a, T, lane, combo_phase<kMode>(warp + kWarps * k));
             C.re[k] = C.ro[k] = 0;
         }
         // Tiles whose columns all exist in both phases skip the column masks (block-uniform).
         // Rows need no mask: the generator writes zero words for bands that do not hold a row.
-        const bool interior = (int64_t)T.u0 + kWords * 32 + (int64_t)(T.i0 + (kIndep ? 0 : 1)) * kPeriod <= a.ncols;
+        const bool interior = (int64_t)T.u0 + kWords * 32 + (int64_t)(T.i0 + (kMode == kModeIndep ? 0 : 1)) * kPeriod <= a.ncols;
         for (int i = tid; i < 5 * kMaxCombos * kWords; i += kTpb) {
             (&S.hist_e[0][0][0])[i] = 0;
             (&S.hist_o[0][0][0])[i] = 0;
+        }
+        // Grouped bands: per band its first area row, swap plane and copy parity.
+        if (kMode == kModeGrouped && tid < kGrpBands) {
+            const int G = a.groups;
+            S.goff[tid] = (tid / G) * (int32_t)kPeriod + (tid % G) * (int32_t)a.row_stride;
+            S.gsw[tid] = kGrpSw + tid % G;
+            S.gflip[tid] = ((tid / G) & 1) ? ~0u : 0u;
         }
         // Row terms of batches 0 and 1 (batch b lives in rows[b % 3]).
         if (tid == 0) {
@@ -851,7 +884,7 @@ __device__ __forceinline__ bool band_tile(BandSmem& S, const BandArgs& a, int64_
                 if (lane == 0) atomicOr(a.overflow, 4u);
             }
             bar_phase ^= 1u << rb;
-            if constexpr (kIndep) {
+            if constexpr (kMode == kModeIndep) {
 #pragma unroll 1
             for (int qq = 0; qq < kGenRows; ++qq) {
                 const int q = gq + qq;
@@ -881,6 +914,65 @@ __device__ __forceinline__ bool band_tile(BandSmem& S, const BandArgs& a, int64_
                     ++m;
                 }
                 for (; m < nb; ++m) clear_plane(dst + m * kPlaneStep);  // rows outside band m
+            }
+            } else if constexpr (kMode == kModeGrouped) {
+#pragma unroll 1
+            for (int qq = 0; qq < kGenRows; ++qq) {
+                const int q = gq + qq;
+                const uint32_t* zr = &S.rows[rb][q * kRowWordsI];
+                const int nv = __shfl_sync(kFull, min((int)zr[kRowValidI], nb), 0);  // warp-uniform
+                uint4* dst = reinterpret_cast<uint4*>(&S.ring[slot][q][0][gw]);
+                constexpr int kPlaneStep = kWords / 4;
+                const int G = a.groups;
+                auto hit = [&](uint32_t x, uint32_t z, uint32_t d) {
+                    const uint32_t t = kMadAdd ? z * one + x : z + x;
+                    return ((t ^ kXorHi) * kMulH + d) < kHitBelow;
+                };
+#pragma unroll 1
+                for (int g = 0; g < G; ++g) {
+                    // Group g: the shared part from the low bits of its row (the same in every copy)
+                    // and, from copy 0's high part, which phase of the pair each copy tests.
+                    const uint32_t zlo = zr[kRowLoI + g];
+                    const uint32_t zpar = (zr[g] ^ kXorHi) & 1u;
+                    uint32_t xa[kGenW], xb[kGenW], dd[kGenW], sw[kGenW];
+#pragma unroll
+                    for (int k = 0; k < kGenW; ++k) {
+                        const Shared sh = shared_part(lox[k], zlo);
+                        const uint32_t pi = (sh.q0 ^ xh0[k] ^ sh.carry ^ zpar) & 1u;
+                        xa[k] = (pi ? xh1[k] : xh0[k]) + sh.carry;
+                        xb[k] = (pi ? xh0[k] : xh1[k]) + sh.carry;
+                        dd[k] = sh.d;
+                        sw[k] = __ballot_sync(kFull, pi != 0);
+                    }
+                    store_plane(dst + (kGrpSw + g) * kPlaneStep, sw);
+                    // Copies c and c + 1: bands m = c G + g and m + G (even copies test the phase
+                    // of xa, odd copies that of xb). Bands from nv on do not hold this row.
+#pragma unroll 1
+                    for (int m = g; m < nb; m += 2 * G) {
+                        const int m1 = m + G;
+                        uint32_t wa[kGenW], wb[kGenW];
+                        if (m1 < nv) {
+                            const uint32_t z0 = zr[m], z1 = zr[m1];
+#pragma unroll
+                            for (int k = 0; k < kGenW; ++k) {
+                                wa[k] = __ballot_sync(kFull, hit(xa[k], z0, dd[k]));
+                                wb[k] = __ballot_sync(kFull, hit(xb[k], z1, dd[k]));
+                            }
+                            store_plane(dst + m * kPlaneStep, wa);
+                            store_plane(dst + m1 * kPlaneStep, wb);
+                        } else {
+                            if (m < nv) {
+                                const uint32_t z0 = zr[m];
+#pragma unroll
+                                for (int k = 0; k < kGenW; ++k) wa[k] = __ballot_sync(kFull, hit(xa[k], z0, dd[k]));
+                                store_plane(dst + m * kPlaneStep, wa);
+                            } else {
+                                clear_plane(dst + m * kPlaneStep);
+                            }
+                            if (m1 < nb) clear_plane(dst + m1 * kPlaneStep);
+                        }
+                    }
+                }
             }
             } else {
 #pragma unroll 1
@@ -969,26 +1061,26 @@ __device__ __forceinline__ bool band_tile(BandSmem& S, const BandArgs& a, int64_
 #pragma unroll
                 for (int t = 0; t < 2; ++t) {
                     if (2 * b + t < 4) continue;  // windows complete from the fifth strip on
-                    if (interior) exact_strip<false, kIndep>(S, a, T, C, 2 * b + t, warp, lane, fx);
-                    else exact_strip<true, kIndep>(S, a, T, C, 2 * b + t, warp, lane, fx);
+                    if (interior) exact_strip<false, kMode>(S, a, T, C, 2 * b + t, warp, lane, fx);
+                    else exact_strip<true, kMode>(S, a, T, C, 2 * b + t, warp, lane, fx);
                 }
                 continue;
             } else {
 #pragma unroll
                 for (int t = 0; t < 2; ++t) {
                     if (interior)
-                        count_strip<false, kIndep, kCands>(S, a, T, C, slot, t, 2 * b + t, warp, lane, fx, lastmask, thr4,
+                        count_strip<false, kMode, kCands>(S, a, T, C, slot, t, 2 * b + t, warp, lane, fx, lastmask, thr4,
                                                            umask, guard, ncand);
                     else
-                        count_strip<true, kIndep, kCands>(S, a, T, C, slot, t, 2 * b + t, warp, lane, fx, lastmask, thr4,
+                        count_strip<true, kMode, kCands>(S, a, T, C, slot, t, 2 * b + t, warp, lane, fx, lastmask, thr4,
                                                           umask, guard, ncand);
                 }
             }
             // Candidates of this batch need rows of batches b-2..b, which stay in the ring until
             // batch b+2 is generated (after the next barrier).
             if (kCands && ncand) {
-                if (interior) flush_cands<false, kIndep>(S, a, T, fx, warp, lane, umask, ncand);
-                else flush_cands<true, kIndep>(S, a, T, fx, warp, lane, umask, ncand);
+                if (interior) flush_cands<false, kMode>(S, a, T, fx, warp, lane, umask, ncand);
+                else flush_cands<true, kMode>(S, a, T, fx, warp, lane, umask, ncand);
                 ncand = 0;
             }
         }
@@ -1003,7 +1095,7 @@ __device__ __forceinline__ bool band_tile(BandSmem& S, const BandArgs& a, int64_
 // union counts per warp (kCands) pays; above it they are rare and are counted at once.
 constexpr int kCandThreshold = 56;
 
-template <bool kMadAdd, bool kIndep, bool kCands, bool kExact = false>
+template <bool kMadAdd, int kMode, bool kCands, bool kExact = false>
 __global__ void __launch_bounds__(kTpb, 1) band_scan_kernel(const BandArgs a) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     BandSmem& S = *reinterpret_cast<BandSmem*>(smem_raw);
@@ -1012,7 +1104,7 @@ __global__ void __launch_bounds__(kTpb, 1) band_scan_kernel(const BandArgs a) {
     uint32_t bar_phase = 0;  // bit r: parity of the next completion of rows_bar[r]
     band_cta_init(S, tid);
     for (int64_t tile = a.tile_begin + blockIdx.x; tile < a.tile_end; tile += gridDim.x)
-        if (!band_tile<kMadAdd, kIndep, kCands, kExact>(S, a, tile, tid, lane, warp, bar_phase)) return;
+        if (!band_tile<kMadAdd, kMode, kCands, kExact>(S, a, tile, tid, lane, warp, bar_phase)) return;
     if (a.hist) {
         __syncthreads();
         for (int i = tid; i < kHistBins; i += kTpb)
@@ -1020,13 +1112,15 @@ __global__ void __launch_bounds__(kTpb, 1) band_scan_kernel(const BandArgs a) {
     }
 }
 
-// Many searches in one persistent launch (each search independent-band or shared-LCG): each CTA
-// takes the next tile of the whole batch from a device counter, finds its search in the tile
-// prefix sums and copies that search's arguments into shared memory. Work item i covers tiles
-// args[i].tile_begin .. + (prefix[i+1] - prefix[i]) of its search. Stale planes of a previous
-// search with more bands are never read by the independent-band counter (it skips combos beyond
-// the band count) and are cleared before a shared-LCG tile.
-template <bool kMadAdd>
+// Many searches of one launch class (band mode, survivor lists, exact counts) in one persistent
+// launch: each CTA takes the next tile of the launch from a device counter, finds its search in
+// the tile prefix sums and copies that search's arguments into shared memory. Work item i covers
+// tiles args[i].tile_begin .. + (prefix[i+1] - prefix[i]) of its search; prefix[0] need not be 0.
+// One class per launch keeps the kernel as lean as the single-search one (no spills). Stale
+// planes of a previous search with more bands are never read by the independent- and grouped-
+// band counters or the exact counts (they skip bands beyond the band count) and are cleared
+// before a shared-LCG tile.
+template <int kMode, bool kCands, bool kExact>
 __global__ void __launch_bounds__(kTpb, 1) band_batch_kernel(const BandArgs* args, const int64_t* prefix,
                                                              int32_t nsearch, unsigned long long* head) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -1035,10 +1129,10 @@ __global__ void __launch_bounds__(kTpb, 1) band_batch_kernel(const BandArgs* arg
     const int warp = __shfl_sync(kFull, tid >> 5, 0);
     uint32_t bar_phase = 0;
     band_cta_init(S, tid);
-    const int64_t total = prefix[nsearch];
+    const int64_t first = prefix[0], total = prefix[nsearch];
     for (;;) {
         if (tid == 0) {
-            const long long t = (long long)atomicAdd(head, 1ull);
+            const long long t = first + (long long)atomicAdd(head, 1ull);
             int lo = 0, hi = nsearch - 1;  // last search whose first tile is <= t
             while (lo < hi) {
                 const int mid = (lo + hi + 1) >> 1;
@@ -1055,18 +1149,7 @@ __global__ void __launch_bounds__(kTpb, 1) band_batch_kernel(const BandArgs* arg
         for (int i = tid; i < kArgWords; i += kTpb)
             reinterpret_cast<uint32_t*>(&S.args)[i] = reinterpret_cast<const uint32_t*>(&args[s])[i];
         __syncthreads();
-        bool ok;
-        if (S.args.exact) {
-            // Exact counts read only the planes of the search's own bands.
-            if (S.args.indep)
-                ok = band_tile<kMadAdd, true, false, true>(S, S.args, S.args.tile_begin + t - prefix[s], tid, lane, warp,
-                                                           bar_phase);
-            else
-                ok = band_tile<kMadAdd, false, false, true>(S, S.args, S.args.tile_begin + t - prefix[s], tid, lane,
-                                                            warp, bar_phase);
-        } else if (S.args.indep) {
-            ok = band_tile<kMadAdd, true, true>(S, S.args, S.args.tile_begin + t - prefix[s], tid, lane, warp, bar_phase);
-        } else {
+        if (kMode == kModeShared && !kExact) {
             // The shared-LCG counter reads every plane: clear planes of bands this search does
             // not generate (a previous search may have left bits there).
             for (int i = tid; i < kRingSlots * kBatchRows * kMaxBands * kWords; i += kTpb) {
@@ -1077,9 +1160,9 @@ __global__ void __launch_bounds__(kTpb, 1) band_batch_kernel(const BandArgs* arg
                 }
             }
             __syncthreads();
-            ok = band_tile<kMadAdd, false, true>(S, S.args, S.args.tile_begin + t - prefix[s], tid, lane, warp, bar_phase);
         }
-        if (!ok) {
+        if (!band_tile<true, kMode, kCands, kExact>(S, S.args, S.args.tile_begin + t - prefix[s], tid, lane, warp,
+                                                     bar_phase)) {
             if (tid == 0) atomicOr(S.args.overflow, 4u);
             return;
         }
@@ -1092,38 +1175,50 @@ __global__ void __launch_bounds__(kTpb, 1) band_batch_kernel(const BandArgs* arg
 // the row lies outside the area plus halo), [kRowLo] = its low 17 bits (the same in every band),
 // [kRowValid] = number of bands of the group that hold the row. Independent records
 // (kRowWordsI): [m] high part, [kRowLoI + m] low 17 bits, [kRowValidI] bands holding the row.
-// Rows v >= vrows (padding) are all zero.
-template <bool kIndep>
+// Grouped bands use the independent layout with band j = c * G + g at input row
+// v + c * 2^17 + g * stride (G * stride = 2^17 when there are several copies, so the bands' rows
+// increase with j and the bands holding a row are a prefix). Rows v >= vrows (padding) are zero.
+template <int kMode>
 __global__ void row_terms_kernel(uint32_t* rt, int32_t vrows_alloc, int32_t vrows, int32_t nj,
                                  int32_t first, int64_t limit, int64_t stride, int64_t seed,
-                                 int32_t use_x_term) {
-    constexpr int kRW = row_words<kIndep>();
-    constexpr int kLo = kIndep ? kRowLoI : kRowLo;
-    constexpr int kValid = kIndep ? kRowValidI : kRowValid;
+                                 int32_t use_x_term, int32_t G) {
+    constexpr bool kSplit = kMode != kModeShared;  // low bits per band
+    constexpr int kRW = row_words<kMode>();
+    constexpr int kLo = kSplit ? kRowLoI : kRowLo;
+    constexpr int kValid = kSplit ? kRowValidI : kRowValid;
     const int32_t groups = (nj + kMaxBands - 1) / kMaxBands;
     const int64_t e = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (e >= (int64_t)groups * vrows_alloc * kRW) return;
     const int32_t w = (int32_t)(e % kRW);
     const int64_t rec = e / kRW;
     const int32_t v = (int32_t)(rec % vrows_alloc), g = (int32_t)(rec / vrows_alloc);
+    auto band_off = [&](int32_t j) -> int64_t {
+        return kMode == kModeGrouped ? (int64_t)(j / G) * kPeriod + (int64_t)(j % G) * stride : (int64_t)j * stride;
+    };
     uint32_t out = 0;
     if (v < vrows) {
         const bool hi = w < kMaxBands;
-        const bool lo = kIndep ? (w >= kLo && w < kLo + kMaxBands) : w == kLo;
+        const bool lo = kSplit ? (w >= kLo && w < kLo + kMaxBands) : w == kLo;
         if (hi || lo) {
-            const int32_t m = hi ? w : kIndep ? w - kLo : 0;
-            const int32_t j = (!kIndep && lo) ? 0 : g * kMaxBands + m;
-            const int64_t off = (int64_t)v + (int64_t)j * stride;
+            const int32_t m = hi ? w : kSplit ? w - kLo : 0;
+            const int32_t j = (!kSplit && lo) ? 0 : g * kMaxBands + m;
+            const int64_t off = (int64_t)v + band_off(j);
             if (j < nj && off < limit) {
                 const int32_t c = (int32_t)((int64_t)first + off);
                 const uint64_t t = (use_x_term ? x_term(c) : z_term(c)) + (uint64_t)seed;
                 out = lo ? (uint32_t)t & 0x1FFFFu : (uint32_t)(t >> kPeriodBits);
             }
         } else if (w == kValid) {
-            // bands j = 32g + m with v + j * stride < limit, capped at the group's size
-            const int64_t jmax = (limit - 1 - v) / stride;  // last band holding the row
-            const int64_t n = min((int64_t)nj, jmax + 1) - (int64_t)g * kMaxBands;
-            out = (uint32_t)max((int64_t)0, min((int64_t)kMaxBands, n));
+            if (kMode == kModeGrouped) {  // one group of at most 16 bands, rows increasing with j
+                int32_t n = 0;
+                while (n < nj && (int64_t)v + band_off(n) < limit) ++n;
+                out = (uint32_t)n;
+            } else {
+                // bands j = 32g + m with v + j * stride < limit, capped at the group's size
+                const int64_t jmax = (limit - 1 - v) / stride;  // last band holding the row
+                const int64_t n = min((int64_t)nj, jmax + 1) - (int64_t)g * kMaxBands;
+                out = (uint32_t)max((int64_t)0, min((int64_t)kMaxBands, n));
+            }
         }
     }
     rt[e] = out;
@@ -1139,76 +1234,120 @@ __global__ void col_terms_kernel(uint64_t* ct, int32_t first, int32_t n, int32_t
 }  // namespace
 
 size_t band_smem_bytes() { return sizeof(BandSmem); }
+
+namespace {
+// The batch kernel of launch class `cls` (band_class): launched over `grid` CTAs, or, with
+// grid == 0, given its dynamic shared-memory size (`prepare_bytes`).
+template <int kMode, bool kCands, bool kExact>
+cudaError_t batch_one(const BandArgs* args, const int64_t* prefix, int32_t n, unsigned long long* head, int grid,
+                      cudaStream_t s, int prepare_bytes) {
+    if (grid == 0)
+        return cudaFuncSetAttribute(band_batch_kernel<kMode, kCands, kExact>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                    prepare_bytes);
+    band_batch_kernel<kMode, kCands, kExact><<<grid, kTpb, sizeof(BandSmem), s>>>(args, prefix, n, head);
+    return cudaGetLastError();
+}
+cudaError_t band_batch_launch(int cls, const BandArgs* args, const int64_t* prefix, int32_t n, unsigned long long* head,
+                              int grid, cudaStream_t s, int prepare_bytes) {
+    switch (cls) {
+        case 0: return batch_one<kModeShared, true, false>(args, prefix, n, head, grid, s, prepare_bytes);
+        case 1: return batch_one<kModeShared, false, false>(args, prefix, n, head, grid, s, prepare_bytes);
+        case 2: return batch_one<kModeIndep, true, false>(args, prefix, n, head, grid, s, prepare_bytes);
+        case 3: return batch_one<kModeIndep, false, false>(args, prefix, n, head, grid, s, prepare_bytes);
+        case 4: return batch_one<kModeGrouped, true, false>(args, prefix, n, head, grid, s, prepare_bytes);
+        case 5: return batch_one<kModeGrouped, false, false>(args, prefix, n, head, grid, s, prepare_bytes);
+        case 6: return batch_one<kModeShared, false, true>(args, prefix, n, head, grid, s, prepare_bytes);
+        case 7: return batch_one<kModeIndep, false, true>(args, prefix, n, head, grid, s, prepare_bytes);
+        case 8: return batch_one<kModeGrouped, false, true>(args, prefix, n, head, grid, s, prepare_bytes);
+        default: return cudaErrorInvalidValue;
+    }
+}
+}  // namespace
 int band_tile_out_w() { return kOutW; }
 int band_max_bands() { return kMaxBands; }
 
-template <bool kMadAdd, bool kIndep, bool kCands, bool kExact = false>
+template <bool kMadAdd, int kMode, bool kCands, bool kExact = false>
 cudaError_t prepare_one(int bytes) {
-    return cudaFuncSetAttribute(band_scan_kernel<kMadAdd, kIndep, kCands, kExact>,
+    return cudaFuncSetAttribute(band_scan_kernel<kMadAdd, kMode, kCands, kExact>,
                                 cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
 }
 
 cudaError_t band_prepare() {
     const int bytes = (int)sizeof(BandSmem);
     cudaError_t e;
-    if ((e = prepare_one<false, false, false>(bytes)) != cudaSuccess || (e = prepare_one<true, false, false>(bytes)) != cudaSuccess ||
-        (e = prepare_one<false, true, false>(bytes)) != cudaSuccess || (e = prepare_one<true, true, false>(bytes)) != cudaSuccess ||
-        (e = prepare_one<false, false, true>(bytes)) != cudaSuccess || (e = prepare_one<true, false, true>(bytes)) != cudaSuccess ||
-        (e = prepare_one<false, true, true>(bytes)) != cudaSuccess || (e = prepare_one<true, true, true>(bytes)) != cudaSuccess ||
-        (e = prepare_one<true, false, false, true>(bytes)) != cudaSuccess ||
-        (e = prepare_one<true, true, false, true>(bytes)) != cudaSuccess ||
-        (e = cudaFuncSetAttribute(band_batch_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes)) != cudaSuccess)
+    if ((e = prepare_one<false, kModeShared, false>(bytes)) != cudaSuccess || (e = prepare_one<true, kModeShared, false>(bytes)) != cudaSuccess ||
+        (e = prepare_one<false, kModeIndep, false>(bytes)) != cudaSuccess || (e = prepare_one<true, kModeIndep, false>(bytes)) != cudaSuccess ||
+        (e = prepare_one<false, kModeShared, true>(bytes)) != cudaSuccess || (e = prepare_one<true, kModeShared, true>(bytes)) != cudaSuccess ||
+        (e = prepare_one<false, kModeIndep, true>(bytes)) != cudaSuccess || (e = prepare_one<true, kModeIndep, true>(bytes)) != cudaSuccess ||
+        (e = prepare_one<true, kModeGrouped, false>(bytes)) != cudaSuccess || (e = prepare_one<true, kModeGrouped, true>(bytes)) != cudaSuccess ||
+        (e = prepare_one<true, kModeShared, false, true>(bytes)) != cudaSuccess ||
+        (e = prepare_one<true, kModeIndep, false, true>(bytes)) != cudaSuccess ||
+        (e = prepare_one<true, kModeGrouped, false, true>(bytes)) != cudaSuccess)
         return e;
-    return cudaFuncSetAttribute(band_batch_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    for (int cls = 0; cls < kBandClasses; ++cls)
+        if ((e = band_batch_launch(cls, nullptr, nullptr, 0, nullptr, 0, nullptr, bytes)) != cudaSuccess) return e;
+    return cudaSuccess;
+}
+
+int band_class(const BandArgs& a) {
+    if (a.exact) return a.indep ? 7 : a.groups ? 8 : 6;
+    const int nc = a.min_size < kCandThreshold ? 0 : 1;
+    return (a.indep ? 2 : a.groups ? 4 : 0) + nc;
 }
 
 cudaError_t launch_band_batch(const BandArgs* args, const int64_t* prefix, int32_t nsearch,
-                              unsigned long long* head, bool mad_add, int grid, cudaStream_t s) {
-    const size_t bytes = sizeof(BandSmem);
-    if (mad_add) band_batch_kernel<true><<<grid, kTpb, bytes, s>>>(args, prefix, nsearch, head);
-    else band_batch_kernel<false><<<grid, kTpb, bytes, s>>>(args, prefix, nsearch, head);
-    return cudaGetLastError();
+                              unsigned long long* head, int cls, int grid, cudaStream_t s) {
+    return band_batch_launch(cls, args, prefix, nsearch, head, grid, s, 0);
 }
 
 cudaError_t launch_band_scan(const BandArgs& a, int grid, cudaStream_t s) {
     const size_t bytes = sizeof(BandSmem);
     if (a.exact) {  // bit-sliced exact counts of every centre (multiply-add band adds)
-        if (a.indep) band_scan_kernel<true, true, false, true><<<grid, kTpb, bytes, s>>>(a);
-        else band_scan_kernel<true, false, false, true><<<grid, kTpb, bytes, s>>>(a);
+        if (a.indep) band_scan_kernel<true, kModeIndep, false, true><<<grid, kTpb, bytes, s>>>(a);
+        else if (a.groups) band_scan_kernel<true, kModeGrouped, false, true><<<grid, kTpb, bytes, s>>>(a);
+        else band_scan_kernel<true, kModeShared, false, true><<<grid, kTpb, bytes, s>>>(a);
         return cudaGetLastError();
     }
     const bool cands = a.min_size < kCandThreshold;
+    if (a.groups) {  // grouped bands (multiply-add band adds)
+        if (cands) band_scan_kernel<true, kModeGrouped, true><<<grid, kTpb, bytes, s>>>(a);
+        else band_scan_kernel<true, kModeGrouped, false><<<grid, kTpb, bytes, s>>>(a);
+        return cudaGetLastError();
+    }
     const int v = (a.mad_add ? 1 : 0) | (a.indep ? 2 : 0) | (cands ? 4 : 0);
     switch (v) {
-        case 0: band_scan_kernel<false, false, false><<<grid, kTpb, bytes, s>>>(a); break;
-        case 1: band_scan_kernel<true, false, false><<<grid, kTpb, bytes, s>>>(a); break;
-        case 2: band_scan_kernel<false, true, false><<<grid, kTpb, bytes, s>>>(a); break;
-        case 3: band_scan_kernel<true, true, false><<<grid, kTpb, bytes, s>>>(a); break;
-        case 4: band_scan_kernel<false, false, true><<<grid, kTpb, bytes, s>>>(a); break;
-        case 5: band_scan_kernel<true, false, true><<<grid, kTpb, bytes, s>>>(a); break;
-        case 6: band_scan_kernel<false, true, true><<<grid, kTpb, bytes, s>>>(a); break;
-        default: band_scan_kernel<true, true, true><<<grid, kTpb, bytes, s>>>(a); break;
+        case 0: band_scan_kernel<false, kModeShared, false><<<grid, kTpb, bytes, s>>>(a); break;
+        case 1: band_scan_kernel<true, kModeShared, false><<<grid, kTpb, bytes, s>>>(a); break;
+        case 2: band_scan_kernel<false, kModeIndep, false><<<grid, kTpb, bytes, s>>>(a); break;
+        case 3: band_scan_kernel<true, kModeIndep, false><<<grid, kTpb, bytes, s>>>(a); break;
+        case 4: band_scan_kernel<false, kModeShared, true><<<grid, kTpb, bytes, s>>>(a); break;
+        case 5: band_scan_kernel<true, kModeShared, true><<<grid, kTpb, bytes, s>>>(a); break;
+        case 6: band_scan_kernel<false, kModeIndep, true><<<grid, kTpb, bytes, s>>>(a); break;
+        default: band_scan_kernel<true, kModeIndep, true><<<grid, kTpb, bytes, s>>>(a); break;
     }
     return cudaGetLastError();
 }
 
-int band_row_words(bool indep) { return indep ? kRowWordsI : kRowWords; }
+int band_row_words(bool split) { return split ? kRowWordsI : kRowWords; }
 
 cudaError_t launch_band_terms(uint64_t* ct, int32_t col_first, int32_t ncols, uint32_t* rt,
                               int32_t vrows_alloc, int32_t vrows, int32_t nj, int32_t row_first,
                               int64_t row_limit, int64_t row_stride, int64_t seed, bool transposed,
-                              bool indep, cudaStream_t s) {
+                              bool indep, int32_t groups, cudaStream_t s) {
     // Columns carry no seed; rows carry it. Transposed searches swap which axis is x.
     col_terms_kernel<<<(ncols + 255) / 256, 256, 0, s>>>(ct, col_first, ncols, transposed ? 0 : 1);
-    const int64_t groups = (nj + kMaxBands - 1) / kMaxBands;
-    const int64_t n = groups * vrows_alloc * band_row_words(indep);
+    const int64_t ngroups = (nj + kMaxBands - 1) / kMaxBands;
+    const int64_t n = ngroups * vrows_alloc * band_row_words(indep || groups > 0);
     const unsigned blocks = (unsigned)((n + 255) / 256);
-    if (indep)
-        row_terms_kernel<true><<<blocks, 256, 0, s>>>(rt, vrows_alloc, vrows, nj, row_first, row_limit,
-                                                       row_stride, seed, transposed ? 1 : 0);
+    if (groups > 0)
+        row_terms_kernel<kModeGrouped><<<blocks, 256, 0, s>>>(rt, vrows_alloc, vrows, nj, row_first, row_limit,
+                                                              row_stride, seed, transposed ? 1 : 0, groups);
+    else if (indep)
+        row_terms_kernel<kModeIndep><<<blocks, 256, 0, s>>>(rt, vrows_alloc, vrows, nj, row_first, row_limit,
+                                                            row_stride, seed, transposed ? 1 : 0, 1);
     else
-        row_terms_kernel<false><<<blocks, 256, 0, s>>>(rt, vrows_alloc, vrows, nj, row_first, row_limit,
-                                                        row_stride, seed, transposed ? 1 : 0);
+        row_terms_kernel<kModeShared><<<blocks, 256, 0, s>>>(rt, vrows_alloc, vrows, nj, row_first, row_limit,
+                                                             row_stride, seed, transposed ? 1 : 0, 1);
     return cudaGetLastError();
 }
 

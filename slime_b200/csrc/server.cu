@@ -93,21 +93,21 @@ void plan_job(Job& j, const Context& c) {
     const int32_t algo = c.engine_for(q);
     const double centres = (double)W * (double)W;
     const double expect = centres * tail_share(q.min_size);
-    j.exact = algo == kAlgoBandExact || algo == kAlgoIndepExact;
+    j.exact = algo_exact(algo);
     j.band = (q.min_size >= 28 || j.exact) && algo != kAlgoGeneral && expect * 1.5 < (double)(16u << 20);
     if (!j.band) {
         // The single search's term tables and hit buffer (library buffers, counted for gating).
         j.bytes = (size_t)(W + 16) * 16 + hit_capacity(q.max_results) * sizeof(Hit);
         return;
     }
-    j.g = band_geometry(W, W, algo != kAlgoBand && algo != kAlgoBandExact, c.sm_count);
+    j.g = band_geometry(W, W, band_mode_of(algo), c.sm_count);
     j.area_x0 = (int32_t)((int64_t)q.center_x - q.rd_max);
     j.area_z0 = (int32_t)((int64_t)q.center_z - q.rd_max);
     j.hit_cap = (uint64_t)std::min<double>((double)(16u << 20), 2.0 * expect + 65536.0);
     const double halo = (double)(W + 16) * (double)(W + 16);
     j.rare_cap = (uint32_t)std::min<double>(1 << 20, 3.0 * halo * rare_share() + 1024.0);
     j.bytes = align256((size_t)(j.g.width_u + 16) * 8) +
-              align256((size_t)j.g.ngroups * j.g.vrows_alloc * band_row_words(j.g.indep) * 4) +
+              align256((size_t)j.g.ngroups * j.g.vrows_alloc * band_row_words(j.g.indep || j.g.groups > 0) * 4) +
               align256((size_t)j.hit_cap * sizeof(Hit)) + align256((size_t)j.rare_cap * sizeof(int2)) + 256;
 }
 
@@ -131,7 +131,7 @@ bool Server::start(Job* j) {
     if (e != cudaSuccess) { c.set_error("server alloc", e); j->mem = nullptr; return false; }
     char* p = (char*)j->mem;
     j->ct = (uint64_t*)p; p += align256((size_t)(j->g.width_u + 16) * 8);
-    j->rt = (uint32_t*)p; p += align256((size_t)j->g.ngroups * j->g.vrows_alloc * band_row_words(j->g.indep) * 4);
+    j->rt = (uint32_t*)p; p += align256((size_t)j->g.ngroups * j->g.vrows_alloc * band_row_words(j->g.indep || j->g.groups > 0) * 4);
     j->hits = (Hit*)p; p += align256((size_t)j->hit_cap * sizeof(Hit));
     j->rare = (int2*)p; p += align256((size_t)j->rare_cap * sizeof(int2));
     j->flags = (unsigned int*)p;
@@ -144,7 +144,7 @@ bool Server::start(Job* j) {
     if ((e = cudaMemsetAsync(p, 0, 256, c.stream)) != cudaSuccess ||
         (e = launch_band_terms(j->ct, col_first, (int32_t)(g.width_u + 16), j->rt, g.vrows_alloc, g.vrows,
                                (int32_t)g.nJ, row_first, g.height_v + 16, g.stride, q.seed, g.transposed, g.indep,
-                               c.stream)) != cudaSuccess ||
+                               g.groups, c.stream)) != cudaSuccess ||
         (e = launch_rare_scan(c.rare_targets.ptr, c.rare_offsets.ptr, q.seed, j->area_z0 - 8, (int32_t)(W + 16),
                               j->area_x0 - 8, (int32_t)(W + 16), j->rare, j->rare_cap, j->flags + 2,
                               c.stream)) != cudaSuccess) {
@@ -233,7 +233,6 @@ bool Server::step(std::vector<Job*>& live) {
     const int64_t floor_tiles = std::max<int64_t>(1, c.sm_count / 4);
     int64_t budget = tiles_per_step;
     std::vector<BandArgs> items;
-    std::vector<int64_t> pre(1, 0);
     std::vector<int64_t> take;
     for (Job* j : band) {
         const int64_t n = std::min<int64_t>(std::max<int64_t>(budget, floor_tiles), j->g.tiles - j->next_tile);
@@ -275,19 +274,16 @@ bool Server::step(std::vector<Job*>& live) {
         a.exact = j->exact ? 1 : 0;
         a.poll_limit = c.wait_polls;
         a.indep = g.indep ? 1 : 0;
+        a.groups = g.groups;
         a.row_stride = g.stride;
         items.push_back(a);
-        pre.push_back(pre.back() + n);
     }
     const int32_t m = (int32_t)items.size();
     cudaError_t e;
     if (m > 0) {
         if ((e = args.reserve((size_t)m)) != cudaSuccess || (e = prefix.reserve((size_t)m + 1)) != cudaSuccess ||
-            (e = head.reserve(1)) != cudaSuccess ||
-            (e = cudaMemcpyAsync(args.ptr, items.data(), (size_t)m * sizeof(BandArgs), cudaMemcpyHostToDevice, c.stream)) != cudaSuccess ||
-            (e = cudaMemcpyAsync(prefix.ptr, pre.data(), ((size_t)m + 1) * sizeof(int64_t), cudaMemcpyHostToDevice, c.stream)) != cudaSuccess ||
-            (e = cudaMemsetAsync(head.ptr, 0, sizeof(unsigned long long), c.stream)) != cudaSuccess ||
-            (e = launch_band_batch(args.ptr, prefix.ptr, m, head.ptr, c.band_mad_add != 0, c.sm_count, c.stream)) != cudaSuccess ||
+            (e = head.reserve(kBandClasses)) != cudaSuccess ||
+            (e = run_band_items(items, args.ptr, prefix.ptr, head.ptr, c.sm_count, c.stream, nullptr)) != cudaSuccess ||
             (e = cudaStreamSynchronize(c.stream)) != cudaSuccess) {
             c.set_error("server step", e);
             return false;

@@ -18,7 +18,8 @@ def grid(indep_from, band_rule):
 def test_derive_recovers_the_crossovers():
     # Shared LCG wins from 48 on 9+ periods and from 54 on 4+ periods.
     rows = grid(44, lambda periods, thr: (periods >= 9 and thr >= 48) or (periods >= 4 and thr >= 54))
-    band_thr, band_periods, fast_thr, fast_periods, indep_thr, indep_centres, ex_thr, ex_centres = derive(rows)
+    band_thr, band_periods, fast_thr, fast_periods, indep_thr, indep_centres, ex_thr, ex_centres, *grp = derive(rows)
+    assert grp[0] == 222  # no grouped timings: the grouped branch is off
     assert ex_thr == 0  # no exact timings: the exact modes are off
     assert indep_thr == 44 and indep_centres == (2 * 30_000 + 1) ** 2
     branches = {(band_thr, band_periods), (fast_thr, fast_periods)}
@@ -42,3 +43,16 @@ def test_derive_exact_modes():
             p["indep_exact_s"] = 0.1 if (p["threshold"] < 46 and p["radius"] >= 100_000) else 3.0
     rule = derive(rows)
     assert rule[6] == 45 and rule[7] == (2 * 100_000 + 1) ** 2  # wins at 44, loses at 46
+
+
+def test_derive_grouped_bands():
+    # Grouped bands win from threshold 50 on areas 1.5-6 periods wide (radius 100k..300k); the
+    # shared LCG keeps the wider areas.
+    rows = grid(44, lambda periods, thr: periods >= 4 and thr >= 48)
+    for p in rows:
+        w = 2 * p["radius"] + 1
+        if PERIOD < w <= 16 * PERIOD:
+            p["grouped_s"] = 0.1 if (p["threshold"] >= 50 and p["radius"] <= 300_000 and p["radius"] >= 100_000) else 5.0
+    rule = derive(rows)
+    assert rule[8:] == [50, 2 * 100_000 + 1, 2 * 300_000 + 1]
+    assert (rule[2], rule[3]) in {(48, 4), (48, 9)} or (rule[0], rule[1]) in {(48, 4), (48, 9)}

@@ -67,9 +67,10 @@ def run(core, mode, *args, **kw):
 
 
 # Engine modes: 2 = shared-LCG band engine, 3 = independent-band engine, 4 / 5 = the same with
-# bit-sliced exact counts of every centre (any threshold).
-ALGO = {2: 200, 3: 300, 4: 210, 5: 310}
-MODES = [2, 3, 4, 5]
+# bit-sliced exact counts of every centre (any threshold), 6 / 7 = grouped bands (X phase pairs with
+# groups of Z period copies), bounded / with exact counts.
+ALGO = {2: 200, 3: 300, 4: 210, 5: 310, 6: 220, 7: 230}
+MODES = [2, 3, 4, 5, 6, 7]
 
 
 @pytest.mark.parametrize("mode", MODES)
@@ -78,7 +79,7 @@ def test_band_engine_search_golden(core, golden, idx, mode):
     g = golden["search"]
     name = str(g["names"][idx])
     seed, rd_max, lo, hi, rd_min, cx, cz, maxr, total = (int(v) for v in g["params"][idx])
-    if mode in (2, 3) and lo < 28:
+    if mode in (2, 3, 6) and lo < 28:
         pytest.skip("the bounded band engines need a threshold of 28 or more")
     got_total, got = run(core, mode, seed, rd_max, lo, hi, rd_min, cx, cz, maxr)
     assert core.lib.get_gpu_v1_algorithm() == ALGO[mode]
@@ -143,7 +144,7 @@ def test_band_vs_general_low_threshold_millions_of_sites(core, mode):
     assert np.array_equal(r_b, r_g)
 
 
-@pytest.mark.parametrize("mode", [4, 5])
+@pytest.mark.parametrize("mode", [4, 5, 7])
 @pytest.mark.parametrize("case", [
     (20240607, 140_000, 40, 221, 0, 0, 0, 2000),             # threshold 40, shared LCG: 2 x 3 bands
     (-4242, 30_000, 36, 44, 5_000, 1_000_000, -3_000, 500),   # low threshold, upper bound, annulus
@@ -185,7 +186,7 @@ def test_annulus_skips_against_the_reference(core, case, mode):
                                    rd_min=rdm, max_results=maxr), total, res, f"annulus mode {mode}")
 
 
-@pytest.mark.parametrize("mode", [2, 3, 5])
+@pytest.mark.parametrize("mode", [2, 3, 5, 6, 7])
 def test_bounded_wait_gives_up_cleanly(core, mode):
     """With a poll limit of 0 the first row-term wait of every CTA gives up: the CTA drains its
     copies in flight and flags the search, which returns -1 with an error text; with the default
@@ -218,7 +219,7 @@ def test_emission_gate_all_engines_agree_and_match_the_reference(core, case):
     gate; totals come from the device histogram (corrected for rare chunks). All engines must give
     the general scan's answer, and the reference GPU library's."""
     t_g, r_g = run(core, 1, *case)
-    for mode in (3, 4, 5):
+    for mode in (3, 4, 5, 6, 7):
         t_b, r_b = run(core, mode, *case)
         assert t_b == t_g, mode
         assert np.array_equal(r_b, r_g), mode
@@ -226,3 +227,25 @@ def test_emission_gate_all_engines_agree_and_match_the_reference(core, case):
     seed, r, lo, hi, rdm, cx, cz, maxr = case
     t_r, r_r = ref_gpu().search(seed, r, lo, hi, rdm, cx, cz, maxr)
     assert t_g == t_r and np.array_equal(r_g, r_r)
+
+
+@pytest.mark.parametrize("case", [
+    (424242, 100_000, 47, 221, 0, 600_000, -600_000, 3000),     # 1.5 periods: 2 copies x 8 groups
+    (-99, 230_000, 52, 221, 0, -1_200_000, 350_000, 2000),      # 3.5 periods: 4 copies x 4 groups
+    (31415, 180_585, 48, 58, 40_000, 123_456, -654_321, 4000),  # 2.8 periods, upper bound + annulus
+    (8, 70_000, 44, 221, 0, 1_800_000, 1_800_000, 1500),        # 1.07 periods at the world border
+])
+def test_grouped_bands_vs_general_and_reference(core, case):
+    """Grouped bands (X phase pairs, groups of Z period copies that share their low bits) must
+    return the general scan's answer and the reference GPU library's."""
+    t_g, r_g = run(core, 1, *case)
+    for mode in (6, 7):
+        t_b, r_b = run(core, mode, *case)
+        assert core.lib.get_gpu_v1_algorithm() == ALGO[mode]
+        assert t_b == t_g, mode
+        assert np.array_equal(r_b, r_g), mode
+    if REF_GPU_SO.exists():
+        from tests.refcheck import ref_gpu
+        seed, r, lo, hi, rdm, cx, cz, maxr = case
+        t_r, r_r = ref_gpu().search(seed, r, lo, hi, rdm, cx, cz, maxr)
+        assert t_b == t_r and np.array_equal(r_b, r_r)

@@ -61,7 +61,7 @@ def test_batch_mixed_requests(core):
                max_results=400),
     ]
     single = singles(core, searches)
-    assert core.lib.get_gpu_v1_algorithm() == 300
+    assert core.lib.get_gpu_v1_algorithm() in (220, 300)  # grouped or independent bands
     batch = core.search_batch(searches)
     check_same(batch, single)
     for i, (q, (total, res)) in enumerate(zip(searches, batch)):
