@@ -9,9 +9,9 @@
  *
  * Results are bit-exact with the reference's arithmetic: every floating-point operation is one
  * IEEE operation in the reference's source order (the library is built without multiply-add
- * contraction). Biome parameter trees are vendored for Minecraft version codes from 1194
- * (1.19.4, 1.20.6, 1.21.4, 1.21.5 and 26.2); a context for an older version code cannot be
- * created (NULL), where the reference also accepts 1180-1193.
+ * contraction). Biome parameter trees are vendored for every version code the reference accepts,
+ * from 1180 (1.18, 1.19.2, 1.19.4, 1.20.6, 1.21.4, 1.21.5 and 26.2); a context for an older
+ * version code cannot be created (NULL), as in the reference.
  *
  * Calls are synchronous and serialised with the library's other entry points.
  */
@@ -95,7 +95,7 @@ void mcgpu_biome20_ctx_destroy(void* handle);
 
 /* mcgpu_modern_ctx_create (MinecraftGPUNoise.cu:1837): a biome context of a Minecraft version
  * code (e.g. 2602 for 26.2) and world seed, for up to `capacity` points per call. NULL for a
- * version code below 1194, capacity <= 0 or no usable device. */
+ * version code below 1180, capacity <= 0 or no usable device. */
 void* mcgpu_modern_ctx_create(int32_t version_code, uint64_t world_seed, int32_t capacity);
 
 /* mcgpu_modern_ctx_create_ex (MinecraftGPUNoise.cu:1966): flags bit 0 = large biomes; other bits

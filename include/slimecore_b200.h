@@ -120,12 +120,12 @@ int64_t slime_b200_last_rare_chunks(void);
 
 /* Engine selection: mode 0 automatic, 1 always the general scan, 2 the shared-LCG band engine,
  * 3 the independent-band engine and 6 the grouped-band engine whenever the threshold allows it
- * (min_size >= 28), 4 / 5 the shared-LCG / independent-band engine with bit-sliced exact counts
- * (any threshold).
+ * (min_size >= 28), 4 / 5 / 7 the shared-LCG / independent-band / grouped-band engine with
+ * bit-sliced exact counts (any threshold).
  * `band_min_threshold` (28..221, other values keep the current one) is the smallest threshold
  * automatic mode sends to the shared-LCG band engine. Results are identical either way; only
  * speed differs. get_gpu_v1_algorithm() reports 100 (general), 200 (band), 300 (independent
- * bands), 210 or 310 (their exact-count modes) or 220 (grouped bands) for the last search. */
+ * bands), 220 (grouped bands), or 210 / 310 / 230 (their exact-count modes) for the last search. */
 void slime_b200_set_engine(int32_t mode, int32_t band_min_threshold);
 
 /* The automatic engine rule as 6, 8 or 11 numbers: {band_min_threshold, band_min_periods,
@@ -133,7 +133,8 @@ void slime_b200_set_engine(int32_t mode, int32_t band_min_threshold);
  * exact_below_threshold, exact_min_centres, grouped_min_threshold, grouped_min_width,
  * grouped_max_width}. Thresholds below exact_below_threshold on areas of
  * exact_min_centres centres or more use the band engines with bit-sliced exact counts (shared LCG
- * on areas band_fast_periods x 2^17 chunks wide, else independent bands) while the expected
+ * on areas band_fast_periods x 2^17 chunks wide, grouped bands from 4 x 2^17 up to
+ * grouped_max_width, else independent bands) while the expected
  * number of sites stays below 1e9. Otherwise grouped bands (X phase pairs with groups of Z period
  * copies) take areas grouped_min_width .. grouped_max_width chunks wide (at most 16 x 2^17) from
  * grouped_min_threshold; the shared-LCG band engine takes areas at least

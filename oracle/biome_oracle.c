@@ -5,7 +5,7 @@
  * function cites the part of the reference (gpu_noise/MinecraftGPUNoise.cu) whose algorithm it
  * restates. Compiled with -ffp-contract=off: every double/float operation is one IEEE operation
  * in source order, as the reference's code reads. The data (octave and climate hashes, octave
- * amplitudes, depth-spline control points, the 26.2 biome parameter tree) comes from
+ * amplitudes, depth-spline control points, the biome parameter trees of 1.18 to 26.2) comes from
  * slime_b200/csrc/biome_data.h; the pin against the reference's own code compiled for the CPU
  * (oracle/_ref/libmcgpu_host_ref.so, golden vectors in tests/golden/biome.npz) checks both the
  * arithmetic and that data.

@@ -36,12 +36,14 @@ OUT = Path(__file__).resolve().parent / "csrc" / "biome_data.h"
 
 # Tree files of the reference and the version codes that select them (mcgpu_select_modern_tree,
 # MinecraftGPUNoise.cu:1785-1820): (name, first version code, family, base). Family 0 is the 1.18 /
-# 1.19.2 tree shape (order 10), family 1 the 1.19.4+ shape (order 6); the library searches any
-# order and depth. The 1.19.4, 1.20.6 and 1.21.4 trees differ from the 1.21.5 tree in at most 100
-# of ~9,100 nodes (same parameter ranges), so they are emitted as patches of it (`base`). The two
-# family-0 trees ("btree18" from 1180, "btree192" from 1192) are not vendored: version codes below
-# 1194 are rejected.
+# 1.19.2 tree shape (order 10, MinecraftGPUNoise.cu:747-788), family 1 the 1.19.4+ shape (order 6,
+# :686-733); both are the same branch-and-bound search, and the library searches any order and
+# depth. The 1.19.4, 1.20.6 and 1.21.4 trees differ from the 1.21.5 tree in at most 100 of ~9,100
+# nodes (same parameter ranges), so they are emitted as patches of it (`base`). Version codes below
+# 1180 are rejected, as the reference rejects them.
 TREES = [
+    ("btree18", 1180, 0, None),
+    ("btree192", 1192, 0, None),
     ("btree215", 1215, 1, None),
     ("btree19", 1194, 1, "btree215"),
     ("btree20", 1206, 1, "btree215"),

@@ -1014,7 +1014,7 @@ void mcgpu_biome20_ctx_destroy(void* handle) {
 }
 
 // Modern biome context (MinecraftGPUNoise.cu:1837-1990): NULL for a version whose tree is not
-// vendored (below 1194), a non-positive capacity or no usable device.
+// vendored (below 1180, as in the reference), a non-positive capacity or no usable device.
 void* mcgpu_modern_ctx_create(int32_t version_code, uint64_t world_seed, int32_t capacity) {
     std::lock_guard<std::mutex> lock(ctx().mu);
     return bm::context_create(version_code, world_seed, 0, capacity);

@@ -11,7 +11,7 @@ Contents (all seeded; world seeds from the 16-seed precise/biome workload):
   perlin_*    single improved-noise samples (seed, x, y, z), a third of them at y = 0
   spline_*    depth-spline values of 4,096 (c, e, pv, w) inputs, as float bits
   c6_*        climate6 {T, H, C, E, depth, W} of 4,096 quarts (normal) and 1,024 (large biomes)
-  bio_*       biome ids of 8,192 quarts, version 26.2, and 2,048 at versions 1.19.4-1.21.5
+  bio_*       biome ids of 8,192 quarts, version 26.2, and 2,048 at versions 1.18-1.21.5
   flt_*       filter masks (flags 3, version 26.2) of 160 candidates: random centres, centres whose
               window holds exactly one Deep Dark quart (border cases) and centres on a slime chunk
               inside Mushroom Fields
@@ -92,7 +92,7 @@ def main():
     out["bio_xyz"] = np.stack([qx, qy, qz], 1)
     out["bio_out"] = ref.biome_at(VERSION, ws, qx, qy, qz)
     out["bio_large_out"] = ref.biome_at(VERSION, ws, qx, qy, qz, 1)
-    vers = np.array([1194, 1206, 1214, 1215], dtype=np.int32)
+    vers = np.array([1180, 1192, 1194, 1206, 1214, 1215], dtype=np.int32)
     out["bio_versions"] = vers
     out["bio_versions_out"] = np.stack([ref.biome_at(int(vv), ws, qx[:2048], qy[:2048], qz[:2048]) for vv in vers])
 

@@ -43,7 +43,7 @@ def test_abi_basics(core):
     lib = core.lib
     assert lib.mcgpu_api_version() == 1
     assert 32 <= lib.mcgpu_modern_recommended_filter_batch() <= 1024
-    assert lib.mcgpu_modern_ctx_create(1180, 1, 16) is None          # tree not vendored
+    assert lib.mcgpu_modern_ctx_create(1179, 1, 16) is None          # before 1.18: no tree
     assert lib.mcgpu_modern_ctx_create(2602, 1, 0) is None           # capacity
     assert lib.mcgpu_modern_ctx_create_ex(2602, 1, 2, 16) is None    # unknown flag
     h = lib.mcgpu_modern_ctx_create(2602, 1, 4)
