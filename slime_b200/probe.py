@@ -11,6 +11,8 @@ under a second):
   exact40     band_scan_kernel, independent bands with bit-sliced exact counts: radius 100,000,
               threshold 40
   band60      band_scan_kernel, shared LCG: radius 600,000 (9+ periods), threshold 60
+  grouped60   band_scan_kernel, grouped bands: radius 200,000 (3 periods: 4 groups x 4 copies),
+              threshold 60
   world60     band_scan_kernel, shared LCG: the full-world threshold-60 scan (36 launches of ~60 ms,
               under 1 GB on the device); profile one launch of it (`-c 1`)
   precise     precise_kernel: precise AFK scores of the best 20,000 sites of a threshold-36 search
@@ -50,6 +52,11 @@ def run(case: str, repeat: int) -> dict:
             total, _ = core.search(SEED, 600_000, 60, 221, 0, 0, 0, 1000)
             out.update(total=int(total), kernel_ms=core.last_search_stats()[0],
                        T_centres_per_s=(2 * 600_000 + 1) ** 2 / core.last_search_stats()[0] / 1e9)
+        elif case == "grouped60":
+            core.lib.slime_b200_set_engine(6, 0)
+            total, _ = core.search(SEED, 200_000, 60, 221, 0, 0, 0, 1000)
+            out.update(total=int(total), kernel_ms=core.last_search_stats()[0],
+                       T_centres_per_s=(2 * 200_000 + 1) ** 2 / core.last_search_stats()[0] / 1e9)
         elif case == "world60":
             from slime_b200 import workloads
             spec = workloads.full_world_scan()
@@ -83,7 +90,7 @@ def run(case: str, repeat: int) -> dict:
 
 def main():
     ap = argparse.ArgumentParser(description=__doc__.split("\n\n")[0])
-    ap.add_argument("case", choices=["general40", "exact40", "band60", "world60", "precise", "biome"])
+    ap.add_argument("case", choices=["general40", "exact40", "band60", "grouped60", "world60", "precise", "biome"])
     ap.add_argument("--repeat", type=int, default=2)
     a = ap.parse_args()
     print(json.dumps(run(a.case, a.repeat)))
