@@ -195,6 +195,7 @@ int32_t Context::search_batch(const SearchSpec* reqs, int32_t n, ExtChunkResult*
     std::vector<uint64_t> emitted(m, 0), counts_h((size_t)m * 2, 0);
     std::vector<uint32_t> flags_h((size_t)m * 4, 0);
     std::vector<Hit> hits_h;
+    std::vector<uint64_t> hoff((size_t)m + 1, 0);  // first host record of each search's sites
     if (m > 0) {
         cudaError_t e;
         // Per search: [0] overflow, [1] fix-up error, [2] rare count, [3] spare; then emitted
@@ -303,12 +304,18 @@ int32_t Context::search_batch(const SearchSpec* reqs, int32_t n, ExtChunkResult*
                 ++last_launches;
             }
         }
-        // One copy of every search's sites (the pool slices are contiguous in search order).
-        uint64_t used = 0;
-        for (int32_t s = 0; s < m; ++s) used = std::max<uint64_t>(used, plan[s].hit_off + std::min(emitted[s], plan[s].hit_cap));
-        hits_h.resize(used);
-        if (used && ((e = cudaMemcpyAsync(hits_h.data(), bt_hits.ptr, used * sizeof(Hit), cudaMemcpyDeviceToHost, stream)) != cudaSuccess ||
-                     (e = cudaStreamSynchronize(stream)) != cudaSuccess)) {
+        // Each search's emitted sites, packed on the host (searches whose slice overflowed run alone).
+        for (int32_t s = 0; s < m; ++s)
+            hoff[s + 1] = hoff[s] + (emitted[s] <= plan[s].hit_cap ? emitted[s] : 0);
+        hits_h.resize(hoff[m]);
+        for (int32_t s = 0; s < m; ++s)
+            if (hoff[s + 1] > hoff[s] &&
+                (e = cudaMemcpyAsync(hits_h.data() + hoff[s], bt_hits.ptr + plan[s].hit_off,
+                                     (hoff[s + 1] - hoff[s]) * sizeof(Hit), cudaMemcpyDeviceToHost, stream)) != cudaSuccess) {
+                set_error("batch copy", e);
+                return -1;
+            }
+        if ((e = cudaStreamSynchronize(stream)) != cudaSuccess) {
             set_error("batch copy", e);
             return -1;
         }
@@ -324,7 +331,7 @@ int32_t Context::search_batch(const SearchSpec* reqs, int32_t n, ExtChunkResult*
             continue;
         }
         std::vector<Hit> best;
-        if (!collect_band(q, p.area_x0, p.area_z0, hits_h.data() + p.hit_off, emitted[s], bt_rare.ptr + p.rare_off,
+        if (!collect_band(q, p.area_x0, p.area_z0, hits_h.data() + hoff[s], emitted[s], bt_rare.ptr + p.rare_off,
                           flags_h[4 * s + 2], bt_counts.ptr + 2 * s + 1, bt_flags.ptr + 4 * s + 1, best, h))
             return -1;
         const int64_t total = finish(q, best, h, results + res_off[p.idx]);
