@@ -128,10 +128,11 @@ int64_t slime_b200_last_rare_chunks(void);
  * bands), 220 (grouped bands), or 210 / 310 / 230 (their exact-count modes) for the last search. */
 void slime_b200_set_engine(int32_t mode, int32_t band_min_threshold);
 
-/* The automatic engine rule as 6, 8 or 11 numbers: {band_min_threshold, band_min_periods,
+/* The automatic engine rule as 6, 8 or 12 numbers: {band_min_threshold, band_min_periods,
  * band_fast_threshold, band_fast_periods, indep_min_threshold, indep_min_centres,
  * exact_below_threshold, exact_min_centres, grouped_min_threshold, grouped_min_width,
- * grouped_max_width}. Thresholds below exact_below_threshold on areas of
+ * grouped_max_width, exact_wide_below_threshold}. Areas 4 x 2^17 chunks wide or more use the
+ * exact counts below the larger of exact_below_threshold and exact_wide_below_threshold. Thresholds below exact_below_threshold on areas of
  * exact_min_centres centres or more use the band engines with bit-sliced exact counts (shared LCG
  * on areas band_fast_periods x 2^17 chunks wide, grouped bands from 4 x 2^17 up to
  * grouped_max_width, else independent bands) while the expected
@@ -141,7 +142,8 @@ void slime_b200_set_engine(int32_t mode, int32_t band_min_threshold);
  * band_min_periods x 2^17 chunks wide from band_min_threshold, or band_fast_periods x 2^17 wide
  * from band_fast_threshold; independent bands take areas of indep_min_centres centres or more from indep_min_threshold; the
  * general scan takes the rest. Thresholds 28..222 (222 disables a branch;
- * exact_below_threshold 0..222, 0 disables it; grouped_min_threshold 28..222), periods 2..64,
+ * exact_below_threshold and exact_wide_below_threshold 0..222, 0 disables them;
+ * grouped_min_threshold 28..222), periods 2..64,
  * widths >= 0. With n = 6 or 8 the numbers not given are kept. Returns 0, or -1 for a wrong count or a value out of range (nothing is changed).
  * slime_b200/autotune.py measures the crossovers on the local GPU and writes them; the defaults are
  * B200 measurements. */

@@ -15,6 +15,7 @@ numbers of slime_b200_set_engine_rule:
   exact_below_threshold, exact_min_centres  exact counts below this threshold on areas this large
   grouped_min_threshold, grouped_min_width, grouped_max_width
                                          grouped bands from this threshold on areas this wide
+  exact_wide_below_threshold             exact counts below this threshold on areas 4+ periods wide
 
 and writes them with the raw timings to a JSON file. SlimeCoreB200 applies that file when it
 loads the library. The general scan's rate does not depend on the area once it fills the GPU, so
@@ -48,6 +49,7 @@ def _time(core, mode, radius, thr, reps=2):
 
 
 GROUPED_MAX_PERIODS = 16  # grouped bands hold at most 16 period copies
+GROUPED_EXACT_MIN_PERIODS = 4  # the library's width from which exact counts may run as grouped bands
 EXACT_MAX_THRESHOLD = 50  # the exact modes are timed up to here (their cost does not depend on it)
 
 
@@ -144,7 +146,7 @@ def derive(rows):
     g = min(g_cands, key=lambda gg: cost(a, b, gg))
     a, b = min(((x, y) for x in cands for y in cands), key=lambda ab: cost(*ab, g))
     return ([a[0], max(2, a[1]), b[0], max(2, b[1]), indep_min_threshold, indep_min_centres] + derive_exact(rows)
-            + [g[0], g[1], g[2]])
+            + [g[0], g[1], g[2], derive_exact_wide(rows)])
 
 
 def derive_exact(rows):
@@ -176,6 +178,26 @@ def derive_exact(rows):
     return [below, min_centres]
 
 
+def derive_exact_wide(rows):
+    """exact_wide_below_threshold: one above the highest threshold up to which the best exact mode
+    beats every other engine on every measured area at least GROUPED_EXACT_MIN_PERIODS wide."""
+    def exact_best(p):
+        return min(p[k] for k in ("indep_exact_s", "band_exact_s", "grouped_exact_s") if k in p)
+
+    def other_best(p):
+        return min(p[k] for k in ("general_s", "indep_s", "band_s", "grouped_s") if k in p)
+
+    pts = [p for p in rows if "indep_exact_s" in p and 2 * p["radius"] + 1 >= GROUPED_EXACT_MIN_PERIODS * PERIOD]
+    below = 0
+    for thr in sorted({p["threshold"] for p in pts}):
+        at = [p for p in pts if p["threshold"] == thr]
+        if all(exact_best(p) < other_best(p) for p in at):
+            below = thr + 1
+        else:
+            break
+    return below
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--out", default=str(DEFAULT_OUT))
@@ -188,13 +210,18 @@ def main():
     core = SlimeCoreB200(apply_tuning=False)
     name = ctypes.create_string_buffer(256)
     core.lib.get_cuda_device_name(name, 256)
-    rows = measure(core, quick=args.quick) if not args.rederive else json.loads(Path(args.out).read_text())["points"]
+    device = name.value.decode(errors="replace")
+    if args.rederive:
+        old = json.loads(Path(args.out).read_text())
+        rows, device = old["points"], old.get("device", device)
+    else:
+        rows = measure(core, quick=args.quick)
     rule = derive(rows)
-    doc = {"device": name.value.decode(errors="replace"),
+    doc = {"device": device,
            "rule": dict(zip(["band_min_threshold", "band_min_periods", "band_fast_threshold",
                              "band_fast_periods", "indep_min_threshold", "indep_min_centres",
                              "exact_below_threshold", "exact_min_centres", "grouped_min_threshold",
-                             "grouped_min_width", "grouped_max_width"], rule)),
+                             "grouped_min_width", "grouped_max_width", "exact_wide_below_threshold"], rule)),
            "seed": SEED, "max_results": 200, "points": rows}
     Path(args.out).write_text(json.dumps(doc, indent=1) + "\n")
     print(json.dumps(doc["rule"]))

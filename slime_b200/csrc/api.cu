@@ -647,13 +647,14 @@ void slime_b200_set_engine(int32_t mode, int32_t band_min_threshold) {
 const char* slime_b200_last_error(void) { return ctx().last_error; }
 
 int32_t slime_b200_set_engine_rule(const int64_t* rule, int32_t n) {
-    if (!rule || (n != 6 && n != 8 && n != 11)) return -1;
+    if (!rule || (n != 6 && n != 8 && n != 12)) return -1;
     const int64_t bt = rule[0], bp = rule[1], ft = rule[2], fp = rule[3], it = rule[4], ic = rule[5];
     const int64_t et = n >= 8 ? rule[6] : ctx().exact_below_threshold, ec = n >= 8 ? rule[7] : ctx().exact_min_centres;
-    const int64_t gt = n == 11 ? rule[8] : ctx().grouped_min_threshold;
-    const int64_t gw = n == 11 ? rule[9] : ctx().grouped_min_width, gx = n == 11 ? rule[10] : ctx().grouped_max_width;
+    const int64_t gt = n == 12 ? rule[8] : ctx().grouped_min_threshold;
+    const int64_t gw = n == 12 ? rule[9] : ctx().grouped_min_width, gx = n == 12 ? rule[10] : ctx().grouped_max_width;
+    const int64_t ew = n == 12 ? rule[11] : ctx().exact_wide_below_threshold;
     if (bt < 28 || bt > 222 || ft < 28 || ft > 222 || it < 28 || it > 222 || bp < 2 || bp > 64 ||
-        fp < 2 || fp > 64 || ic < 0 || et < 0 || et > 222 || ec < 0 || gt < 28 || gt > 222 || gw < 0 || gx < 0)
+        fp < 2 || fp > 64 || ic < 0 || et < 0 || et > 222 || ec < 0 || gt < 28 || gt > 222 || gw < 0 || gx < 0 || ew < 0 || ew > 222)
         return -1;
     std::lock_guard<std::mutex> lock(ctx().mu);
     slime::Context& c = ctx();
@@ -668,11 +669,12 @@ int32_t slime_b200_set_engine_rule(const int64_t* rule, int32_t n) {
     c.grouped_min_threshold = (int32_t)gt;
     c.grouped_min_width = gw;
     c.grouped_max_width = gx;
+    c.exact_wide_below_threshold = (int32_t)ew;
     return 0;
 }
 
 int32_t slime_b200_get_engine_rule(int64_t* rule, int32_t n) {
-    if (!rule || (n != 6 && n != 8 && n != 11)) return -1;
+    if (!rule || (n != 6 && n != 8 && n != 12)) return -1;
     std::lock_guard<std::mutex> lock(ctx().mu);
     const slime::Context& c = ctx();
     rule[0] = c.band_min_threshold;
@@ -685,10 +687,11 @@ int32_t slime_b200_get_engine_rule(int64_t* rule, int32_t n) {
         rule[6] = c.exact_below_threshold;
         rule[7] = c.exact_min_centres;
     }
-    if (n == 11) {
+    if (n == 12) {
         rule[8] = c.grouped_min_threshold;
         rule[9] = c.grouped_min_width;
         rule[10] = c.grouped_max_width;
+        rule[11] = c.exact_wide_below_threshold;
     }
     return 0;
 }

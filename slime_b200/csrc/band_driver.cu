@@ -53,7 +53,9 @@ int32_t Context::engine_for(const SearchSpec& q) const {
     // Low thresholds: exact counts of every centre, while the sites stay few enough to collect
     // (the band engines emit every site in range; the general scan gates by count on the device).
     constexpr double kExactMaxSites = 1e9;
-    if (q.min_size < exact_below_threshold && w * w >= exact_min_centres &&
+    const int32_t exact_below =
+        w >= kGroupedExactMinPeriods * kP ? std::max(exact_below_threshold, exact_wide_below_threshold) : exact_below_threshold;
+    if (q.min_size < exact_below && w * w >= exact_min_centres &&
         (double)w * (double)w * tail_share(q.min_size) <= kExactMaxSites)
         // Exact counts cost the same per centre in every mode; the generator's sharing decides:
         // independent bands on narrow areas, grouped bands from 4 periods (measured on B200:

@@ -157,6 +157,9 @@ struct Context {
     // Grouped bands for areas grouped_min_width .. grouped_max_width chunks wide (at most
     // kGroupedMaxPeriods periods) from grouped_min_threshold, before the shared-LCG rule.
     int32_t grouped_min_threshold = 46;
+    // Areas kGroupedExactMinPeriods periods wide or more use exact counts below this threshold
+    // instead (their exact modes share more of the generator's work).
+    int32_t exact_wide_below_threshold = 45;
     int64_t grouped_min_width = 200001;
     int64_t grouped_max_width = 2000001;
     int64_t last_rare = 0;             // rare redraw chunks found by the last band search

@@ -128,7 +128,7 @@ class SlimeError(RuntimeError):
 TUNING = Path(__file__).with_name("tuning_b200.json")
 RULE_KEYS = ("band_min_threshold", "band_min_periods", "band_fast_threshold", "band_fast_periods",
              "indep_min_threshold", "indep_min_centres", "exact_below_threshold", "exact_min_centres",
-             "grouped_min_threshold", "grouped_min_width", "grouped_max_width")
+             "grouped_min_threshold", "grouped_min_width", "grouped_max_width", "exact_wide_below_threshold")
 
 
 class SlimeCoreB200:
@@ -142,7 +142,7 @@ class SlimeCoreB200:
             self.set_engine_rule(json.loads(TUNING.read_text())["rule"])
 
     def set_engine_rule(self, rule: dict):
-        keys = next(RULE_KEYS[:n] for n in (11, 8, 6) if all(k in rule for k in RULE_KEYS[:n]))
+        keys = next(RULE_KEYS[:n] for n in (12, 8, 6) if all(k in rule for k in RULE_KEYS[:n]))
         vals = np.array([int(rule[k]) for k in keys], dtype=np.int64)
         self._check(self.lib.slime_b200_set_engine_rule(_ptr(vals), len(vals)) == 0, "set_engine_rule")
 

@@ -54,5 +54,17 @@ def test_derive_grouped_bands():
         if PERIOD < w <= 16 * PERIOD:
             p["grouped_s"] = 0.1 if (p["threshold"] >= 50 and p["radius"] <= 300_000 and p["radius"] >= 100_000) else 5.0
     rule = derive(rows)
-    assert rule[8:] == [50, 2 * 100_000 + 1, 2 * 300_000 + 1]
+    assert rule[8:11] == [50, 2 * 100_000 + 1, 2 * 300_000 + 1]
     assert (rule[2], rule[3]) in {(48, 4), (48, 9)} or (rule[0], rule[1]) in {(48, 4), (48, 9)}
+
+
+def test_derive_exact_wide():
+    # Exact counts win below 46 on areas 4+ periods wide (radius 300k and up), below 42 elsewhere.
+    rows = grid(40, lambda periods, thr: periods >= 9 and thr >= 48)
+    for p in rows:
+        if p["threshold"] <= 50:
+            wide = 2 * p["radius"] + 1 >= 4 * PERIOD
+            p["indep_exact_s"] = 0.1 if (p["threshold"] < (46 if wide else 42)) else 3.0
+    rule = derive(rows)
+    assert rule[11] == 45  # wins at 44, loses at the next measured threshold (46)
+    assert rule[6] == 41
