@@ -308,8 +308,11 @@ __global__ void __launch_bounds__(kThreads) insert_kernel(int64_t seed, const in
 
 // Verdict bits of the quart columns of unique chunks: bit 0 Deep Dark at some quart Y -16..0,
 // bit 1 Mushroom Fields at quart Y 16. NQ queries: 18 (both), 17 (Deep Dark), 1 (Mushroom).
+// Four CTAs per SM (128 registers, no spills): the traversal is latency-bound; twice the warps of
+// the register-limited default (200 registers) ran 23 % more quart columns per second on B200 in a
+// back-to-back comparison on one GPU.
 template <int NQ>
-__global__ void __launch_bounds__(kThreads) chunk_kernel(const Climate* __restrict__ cl, const SplineHead* heads,
+__global__ void __launch_bounds__(kThreads, 4) chunk_kernel(const Climate* __restrict__ cl, const SplineHead* heads,
                                                          const SplinePt* pts, const uint64_t* __restrict__ nodes,
                                                          const int2* __restrict__ param, TreeGeom g,
                                                          const int2* __restrict__ chunks, int32_t nchunks,
