@@ -628,8 +628,9 @@ __host__ __device__ constexpr int column_half_height(int dx) {
 // Counts of the windows starting one row lower than `cnt` (window start DZ - 1 -> DZ among the
 // rows R / next-word rows Rn): per column one cell enters (row DZ + 8 + H) and one leaves (row
 // DZ + 7 - H), so count' = count + entering - leaving (mod 256, exact since counts are 0..221).
+// DZ = 0 reads row -1 (R[-1], Rn[-1] must exist).
 template <int DZ>
-__device__ __forceinline__ void bs_slide(const uint32_t (&R)[20], const uint32_t (&Rn)[20], uint32_t (&cnt)[8]) {
+__device__ __forceinline__ void bs_slide(const uint32_t* R, const uint32_t* Rn, uint32_t (&cnt)[8]) {
     uint32_t in[17], out[17];
 #pragma unroll
     for (int dx = 0; dx < 17; ++dx) {
@@ -689,7 +690,12 @@ __device__ __forceinline__ void exact_strip(BandSmem& S, const BandArgs& a, cons
         const int combo = warp + kWarps * k;
         const int m = combo_band<kMode>(combo), ph = combo_phase<kMode>(combo);
         if (m >= a.nb) continue;  // warp-uniform: planes of bands beyond the count are empty
-        uint32_t R[20];
+        // Rows r0 - 1 .. r0 + 19 of the combo (row r0 - 1 only when the strip slides on from the
+        // previous one; its batch may already be overwritten in the ring, so it comes from what the
+        // previous strip saved).
+        uint32_t Rx[21], Rnx[21];
+        uint32_t* const R = Rx + 1;
+        uint32_t* const Rn = Rnx + 1;
 #pragma unroll
         for (int i = 0; i < 20; ++i) {
             uint32_t w = combo_word<kMode>(S, r0 + i, combo, fx, lane);
@@ -706,10 +712,22 @@ __device__ __forceinline__ void exact_strip(BandSmem& S, const BandArgs& a, cons
         const int64_t band_v = band_row0<kMode>(S, a, m);
         // The next word's rows (lane 31 gets its own back: only its centres 16+, which lie beyond
         // the tile's output columns, would read them).
-        uint32_t Rn[20];
 #pragma unroll
         for (int i = 0; i < 20; ++i) Rn[i] = __shfl_down_sync(kFull, R[i], 1);
         uint32_t cnt[8];
+        // Strips after a tile's first continue from the previous strip's last window row: its 8
+        // count planes and its row 3 (this strip's row -1) wait in the box-sum history, which the
+        // exact modes do not use (9 words per combo and lane).
+        uint32_t* const saved = &S.hist_e[0][0][0] + (size_t)combo * 9 * kWords + lane;
+        const bool slide_in = st > 4 && a.rd_min_sq == 0;
+        if (slide_in) {
+#pragma unroll
+            for (int i = 0; i < 8; ++i) cnt[i] = saved[i * kWords];
+            Rx[0] = saved[8 * kWords];
+        } else {
+            Rx[0] = 0u;
+        }
+        Rnx[0] = __shfl_down_sync(kFull, Rx[0], 1);
         // Annulus searches: skip the strip when all of its centres lie inside the rd_min disc
         // (warp-uniform: the strip's 4 rows across the tile's output columns).
         if (a.rd_min_sq) {
@@ -726,9 +744,11 @@ __device__ __forceinline__ void exact_strip(BandSmem& S, const BandArgs& a, cons
             const int rr = r0 + dz;  // window start row = centre row index in the tile
             const int64_t v = (int64_t)T.v0 + rr;
             const bool rowok = rr < T.out_h && v + band_v < a.height_v;
-            // The strip's first window row is counted in full; the next three slide down a row.
-            if (dz == 0) bs_window_counts<0>(R, cnt);
-            else if (dz == 1) bs_slide<1>(R, Rn, cnt);
+            // A tile's first window row is counted in full; every later one slides down a row.
+            if (dz == 0) {
+                if (slide_in) bs_slide<0>(R, Rn, cnt);
+                else bs_window_counts<0>(*reinterpret_cast<const uint32_t(*)[20]>(R), cnt);
+            } else if (dz == 1) bs_slide<1>(R, Rn, cnt);
             else if (dz == 2) bs_slide<2>(R, Rn, cnt);
             else bs_slide<3>(R, Rn, cnt);
             uint32_t pass = rowok ? colok & bs_at_least(cnt, a.min_size) : 0u;
@@ -770,6 +790,11 @@ __device__ __forceinline__ void exact_strip(BandSmem& S, const BandArgs& a, cons
                 const int32_t cz = (int32_t)(a.transposed ? a.area_z0 + cu : a.area_z0 + cv);
                 if (base < a.cap) a.out[base] = Hit{bs_value(cnt, j), cx, cz};
             }
+        }
+        if (a.rd_min_sq == 0) {  // for the next strip of the tile
+#pragma unroll
+            for (int i = 0; i < 8; ++i) saved[i * kWords] = cnt[i];
+            saved[8 * kWords] = R[3];
         }
     }
 }
