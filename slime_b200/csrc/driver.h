@@ -152,7 +152,7 @@ struct Context {
     // Below exact_below_threshold, areas of exact_min_centres centres or more use the band engines
     // with bit-sliced exact counts (shared LCG on areas band_fast_periods periods wide, else
     // independent bands), as long as the expected number of sites stays below kExactMaxSites.
-    int32_t exact_below_threshold = 43;
+    int32_t exact_below_threshold = 45;
     int64_t exact_min_centres = 400040001;
     // Grouped bands for areas grouped_min_width .. grouped_max_width chunks wide (at most
     // kGroupedMaxPeriods periods) from grouped_min_threshold, before the shared-LCG rule.
