@@ -95,6 +95,11 @@ class ClockSampler:
                 "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
                 "samples": len(self.samples)}
 
+    def median_sm_hz(self) -> float:
+        """Median SM clock seen under load (Hz); the B200's maximum when nothing was sampled."""
+        mhz = self.summary().get("sm_mhz")
+        return (mhz or 1965.0) * 1e6
+
 
 def int_peak(core):
     """Measured INT32 lane-op peak: the best of the integer probes (single forms and the two
@@ -536,7 +541,11 @@ def main():
                                     "LOP3/IADD3/IMAD/generator-mix probes",
                      "traffic_note": "DRAM bytes of one full-world band_scan_kernel launch "
                                      "(ncu capture)",
-                     "probes_T_lane_ops": {k: v / 1e12 for k, v in rates.items()}},
+                     "probes_T_lane_ops": {k: v / 1e12 for k, v in rates.items()},
+                     # The same achieved rate against the nominal INT32 issue rate of the clock
+                     # the run saw (148 SMs x 128 lanes per clock).
+                     "frac_of_nominal_int32_issue": achieved_ops / (148 * 128 * sampler.median_sm_hz()),
+                     "nominal_int32_issue_T_lane_ops": 148 * 128 * sampler.median_sm_hz() / 1e12},
         "clocks": sampler.summary(),
     }
     if world == 1 and not args.no_cpu_baseline:
