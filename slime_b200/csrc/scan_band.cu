@@ -1191,6 +1191,15 @@ __global__ void __launch_bounds__(kTpb, 1) band_batch_kernel(const BandArgs* arg
             if (tid == 0) atomicOr(S.args.overflow, 4u);
             return;
         }
+        // The tile's search keeps a count histogram: add this tile's counts to it (band_tile ended
+        // with a barrier) and clear them before the next tile, which may be another search's.
+        if (S.args.hist) {
+            for (int i = tid; i < kHistBins; i += kTpb)
+                if (S.hist[i]) {
+                    atomicAdd(&S.args.hist[i], S.hist[i]);
+                    S.hist[i] = 0;
+                }
+        }
     }
 }
 

@@ -55,7 +55,13 @@ struct Job {
     int2* rare = nullptr;
     unsigned int* flags = nullptr;            // overflow, fix-up error, rare count, spare
     unsigned long long* counts = nullptr;     // emitted, fixed
+    // Count histogram of every centre in range and its rare-chunk correction (2 x kHistBins), and
+    // the emission gate: only centres from emit_min on are written to the hit slice.
+    unsigned int* hist = nullptr;
+    int32_t emit_min = 0;
 };
+
+constexpr uint64_t kServerHitCap = 16u << 20;  // hit records of one job's slice at most
 
 size_t align256(size_t n) { return (n + 255) & ~(size_t)255; }
 
@@ -81,7 +87,8 @@ struct Server {
     bool step(std::vector<Job*>& live);
     void complete(Job* j, int64_t total, bool ok);
     bool start(Job* j);
-    bool finish_band(Job* j);
+    // 1 finished, 0 failed, 2 to be rescanned with a lower emission gate.
+    int finish_band(Job* j);
 };
 
 namespace {
@@ -92,9 +99,18 @@ void plan_job(Job& j, const Context& c) {
     const int64_t W = 2 * q.rd_max + 1;
     const int32_t algo = c.engine_for(q);
     const double centres = (double)W * (double)W;
-    const double expect = centres * tail_share(q.min_size);
+    // Emission gate, as the single search chooses it: the smallest count whose expected number of
+    // centres fits an eighth of the largest slice while still covering the ranked results
+    // (biome requests keep more, as the single search does) four times over.
+    const int64_t want = (q.biome_flags & 3) ? 2LL * q.max_results + 1024 : (int64_t)q.max_results;
+    int32_t emit = q.min_size;
+    while (emit < q.max_size && centres * tail_share(emit) > (double)kServerHitCap / 8.0 &&
+           centres * tail_share(emit + 1) >= 4.0 * (double)want)
+        ++emit;
+    j.emit_min = emit;
+    const double expect = centres * tail_share(emit);
     j.exact = algo_exact(algo);
-    j.band = (q.min_size >= 28 || j.exact) && algo != kAlgoGeneral && expect * 1.5 < (double)(16u << 20);
+    j.band = (q.min_size >= 28 || j.exact) && algo != kAlgoGeneral && expect * 1.5 < (double)kServerHitCap;
     if (!j.band) {
         // The single search's term tables and hit buffer (library buffers, counted for gating).
         j.bytes = (size_t)(W + 16) * 16 + hit_capacity(q.max_results) * sizeof(Hit);
@@ -108,7 +124,8 @@ void plan_job(Job& j, const Context& c) {
     j.rare_cap = (uint32_t)std::min<double>(1 << 20, 3.0 * halo * rare_share() + 1024.0);
     j.bytes = align256((size_t)(j.g.width_u + 16) * 8) +
               align256((size_t)j.g.ngroups * j.g.vrows_alloc * band_row_words(j.g.indep || j.g.groups > 0) * 4) +
-              align256((size_t)j.hit_cap * sizeof(Hit)) + align256((size_t)j.rare_cap * sizeof(int2)) + 256;
+              align256((size_t)j.hit_cap * sizeof(Hit)) + align256((size_t)j.rare_cap * sizeof(int2)) +
+              align256(2 * kHistBins * sizeof(unsigned int)) + 256;
 }
 
 }  // namespace
@@ -134,6 +151,7 @@ bool Server::start(Job* j) {
     j->rt = (uint32_t*)p; p += align256((size_t)j->g.ngroups * j->g.vrows_alloc * band_row_words(j->g.indep || j->g.groups > 0) * 4);
     j->hits = (Hit*)p; p += align256((size_t)j->hit_cap * sizeof(Hit));
     j->rare = (int2*)p; p += align256((size_t)j->rare_cap * sizeof(int2));
+    j->hist = (unsigned int*)p; p += align256(2 * kHistBins * sizeof(unsigned int));
     j->flags = (unsigned int*)p;
     j->counts = (unsigned long long*)(p + 32);
     const SearchSpec& q = j->q;
@@ -142,6 +160,7 @@ bool Server::start(Job* j) {
     const int32_t col_first = (g.transposed ? j->area_z0 : j->area_x0) - 8;
     const int32_t row_first = (g.transposed ? j->area_x0 : j->area_z0) - 8;
     if ((e = cudaMemsetAsync(p, 0, 256, c.stream)) != cudaSuccess ||
+        (e = cudaMemsetAsync(j->hist, 0, 2 * kHistBins * sizeof(unsigned int), c.stream)) != cudaSuccess ||
         (e = launch_band_terms(j->ct, col_first, (int32_t)(g.width_u + 16), j->rt, g.vrows_alloc, g.vrows,
                                (int32_t)g.nJ, row_first, g.height_v + 16, g.stride, q.seed, g.transposed, g.indep,
                                g.groups, c.stream)) != cudaSuccess ||
@@ -155,7 +174,7 @@ bool Server::start(Job* j) {
     return true;
 }
 
-bool Server::finish_band(Job* j) {
+int Server::finish_band(Job* j) {
     Context& c = ctx();
     uint32_t fl[4] = {0, 0, 0, 0};
     unsigned long long cnt[2] = {0, 0};
@@ -164,41 +183,121 @@ bool Server::finish_band(Job* j) {
         (e = cudaMemcpyAsync(cnt, j->counts, sizeof(cnt), cudaMemcpyDeviceToHost, c.stream)) != cudaSuccess ||
         (e = cudaStreamSynchronize(c.stream)) != cudaSuccess) {
         c.set_error("server finish", e);
-        return false;
+        return 0;
     }
-    if (fl[0] & 4u) { c.set_error("band engine: row-term copy timed out", cudaErrorLaunchTimeout); return false; }
+    if (fl[0] & 4u) { c.set_error("band engine: row-term copy timed out", cudaErrorLaunchTimeout); return 0; }
     j->results.assign((size_t)std::max<int32_t>(1, j->q.max_results), ExtChunkResult{});
     if ((fl[0] & 1u) || cnt[0] > j->hit_cap || fl[2] > j->rare_cap) {
         // A dense strip, a full hit slice or too many rare chunks: the single search redoes it.
         if (j->mem) cudaFreeAsync(j->mem, c.stream);
         j->mem = nullptr;
         const int64_t t = c.search(j->q, j->results.data());
-        if (t < 0) return false;
+        if (t < 0) return 0;
         j->total = t;
-        return true;
+        return 1;
     }
     const uint64_t n = cnt[0];
     const uint32_t nrare = fl[2];
     std::vector<Hit> hits_h(n);
     if (n && nrare && (e = launch_filter_hits(j->hits, (int64_t)n, j->rare, (int32_t)nrare, false, c.stream)) != cudaSuccess) {
         c.set_error("server filter", e);
-        return false;
+        return 0;
     }
     if (n && ((e = cudaMemcpyAsync(hits_h.data(), j->hits, n * sizeof(Hit), cudaMemcpyDeviceToHost, c.stream)) != cudaSuccess ||
               (e = cudaStreamSynchronize(c.stream)) != cudaSuccess)) {
         c.set_error("server copy", e);
-        return false;
+        return 0;
     }
     std::vector<Hit> best;
+    best.reserve(n);
+    for (const Hit& hit : hits_h)
+        if (hit.count >= 0) best.push_back(hit);  // window holds a rare chunk: fixed below
+    // Exact counts of the centres around the rare chunks, and the histogram's correction (their
+    // first-draw counts out, their exact counts in).
+    int* delta = reinterpret_cast<int*>(j->hist + kHistBins);
+    if (nrare) {
+        if ((e = c.fixed.reserve(1u << 20)) != cudaSuccess) {
+            c.set_error("server fixup", e);
+            return 0;
+        }
+        FixArgs f{};
+        f.area_x0 = j->area_x0;
+        f.area_z0 = j->area_z0;
+        f.width = 2 * j->q.rd_max + 1;
+        f.height = 2 * j->q.rd_max + 1;
+        f.rd_min_sq = j->q.rd_min * j->q.rd_min;
+        f.center_x = j->q.center_x;
+        f.center_z = j->q.center_z;
+        f.min_size = j->q.min_size;
+        f.max_size = j->q.max_size;
+        f.fixed = c.fixed.ptr;
+        f.fixed_count = j->counts + 1;
+        f.cap = c.fixed.count;
+        f.error = j->flags + 1;
+        f.hist_delta = delta;
+        uint64_t nf = 0;
+        uint32_t ferr = 0;
+        if ((e = cudaMemsetAsync(j->counts + 1, 0, 8, c.stream)) != cudaSuccess ||
+            (e = cudaMemsetAsync(j->flags + 1, 0, 4, c.stream)) != cudaSuccess ||
+            (e = cudaMemsetAsync(delta, 0, kHistBins * sizeof(int), c.stream)) != cudaSuccess ||
+            (e = launch_fixup(j->rare, (int32_t)nrare, j->q.seed, f, c.stream)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(&nf, j->counts + 1, 8, cudaMemcpyDeviceToHost, c.stream)) != cudaSuccess ||
+            (e = cudaMemcpyAsync(&ferr, j->flags + 1, 4, cudaMemcpyDeviceToHost, c.stream)) != cudaSuccess ||
+            (e = cudaStreamSynchronize(c.stream)) != cudaSuccess) {
+            c.set_error("server fixup", e);
+            return 0;
+        }
+        if (nf > c.fixed.count || ferr) { c.set_error("fixup overflow", cudaErrorUnknown); return 0; }
+        const size_t old = best.size();
+        best.resize(old + nf);
+        if (nf && ((e = cudaMemcpyAsync(best.data() + old, c.fixed.ptr, nf * sizeof(Hit), cudaMemcpyDeviceToHost,
+                                        c.stream)) != cudaSuccess ||
+                   (e = cudaStreamSynchronize(c.stream)) != cudaSuccess)) {
+            c.set_error("server copy", e);
+            return 0;
+        }
+    }
+    // Every centre in range by count, from the device histogram with the rare-chunk correction.
+    std::vector<uint32_t> hd(2 * kHistBins, 0u);
+    if ((e = cudaMemcpyAsync(hd.data(), j->hist, hd.size() * sizeof(uint32_t), cudaMemcpyDeviceToHost, c.stream)) != cudaSuccess ||
+        (e = cudaStreamSynchronize(c.stream)) != cudaSuccess) {
+        c.set_error("server histogram", e);
+        return 0;
+    }
     std::vector<uint32_t> h(kHistBins, 0u);
-    if (!c.collect_band(j->q, j->area_x0, j->area_z0, hits_h.data(), n, j->rare, nrare, j->counts + 1, j->flags + 1,
-                        best, h))
-        return false;
+    for (int i = 0; i < kHistBins; ++i) h[i] = (uint32_t)((int64_t)hd[i] + (int32_t)hd[kHistBins + i]);
+    uint64_t total = 0, have = 0;
+    for (int k = j->q.min_size; k <= j->q.max_size; ++k) {
+        total += h[k];
+        if (k >= j->emit_min) have += h[k];
+    }
+    const int64_t want = (j->q.biome_flags & 3) ? 2LL * j->q.max_results + 1024 : (int64_t)j->q.max_results;
+    const uint64_t need = std::min<uint64_t>(total, (uint64_t)want);
+    if (have < need && j->emit_min > j->q.min_size) {
+        // Too few sites sent: rescan with the exact gate (the highest count whose cumulative number
+        // covers need), like the single search's second pass.
+        uint64_t acc = 0;
+        int32_t gate = j->q.max_size;
+        for (int k = j->q.max_size; k >= j->q.min_size; --k) {
+            acc += h[k];
+            gate = k;
+            if (acc >= need) break;
+        }
+        j->emit_min = gate;
+        j->next_tile = 0;
+        if ((e = cudaMemsetAsync(j->counts, 0, 2 * sizeof(unsigned long long), c.stream)) != cudaSuccess ||
+            (e = cudaMemsetAsync(j->flags, 0, 2 * sizeof(unsigned int), c.stream)) != cudaSuccess ||
+            (e = cudaMemsetAsync(j->hist, 0, 2 * kHistBins * sizeof(unsigned int), c.stream)) != cudaSuccess) {
+            c.set_error("server rescan", e);
+            return 0;
+        }
+        return 2;
+    }
     int64_t t = c.finish(j->q, best, h, j->results.data());
     if (t == kNeedMoreSites) t = c.search(j->q, j->results.data());  // biome exclusion needs more sites
-    if (t < 0) return false;
+    if (t < 0) return 0;
     j->total = t;
-    return true;
+    return 1;
 }
 
 // One step over the live jobs (called with the library lock held).
@@ -276,6 +375,8 @@ bool Server::step(std::vector<Job*>& live) {
         a.indep = g.indep ? 1 : 0;
         a.groups = g.groups;
         a.row_stride = g.stride;
+        a.hist = j->hist;
+        a.emit_min = j->emit_min;
         items.push_back(a);
     }
     const int32_t m = (int32_t)items.size();
@@ -293,8 +394,9 @@ bool Server::step(std::vector<Job*>& live) {
         Job* j = band[k];
         j->next_tile += std::max<int64_t>(0, take[k]);
         if (j->next_tile < j->g.tiles) continue;
-        const bool ok = finish_band(j);
-        complete(j, ok ? j->total : -1, ok);
+        const int r = finish_band(j);
+        if (r == 2) continue;  // its tiles run again with a lower emission gate
+        complete(j, r == 1 ? j->total : -1, r == 1);
     }
     return true;
 }

@@ -126,3 +126,25 @@ def test_server_destroy_with_requests_in_flight(core):
     q = MIX[1]
     t_s, r_s = single(core, q)
     assert t_s >= 0 and len(r_s) == min(t_s, q.max_results)
+
+
+def test_server_gated_low_threshold_requests(core):
+    """Requests with tens of millions of sites in range (thresholds 40-44 on wide areas) run in the
+    batch kernel with an emission gate: only centres at or above it are sent, the totals come
+    from the device histogram (rare-chunk corrected), and a gate that proves too high triggers a
+    second pass. Results must be the single search's, beside small requests in the same steps."""
+    from slime_b200.lib import SlimeServer
+    reqs = [
+        Search(seed=91, center_x=100_000, center_z=-250_000, radius=300_000, min_size=40, max_results=2000),
+        Search(seed=-92, center_x=0, center_z=0, radius=200_000, min_size=42, max_size=47, max_results=500),
+        Search(seed=93, center_x=-1_000_000, center_z=5_000, radius=250_000, min_size=44, rd_min=120_000,
+               max_results=50_000),
+        Search(seed=94, center_x=3, center_z=-3, radius=2_500, min_size=45, max_results=100),
+    ]
+    with SlimeServer(core=core) as server:
+        got = run_all(server, reqs)
+    for i, (q, (total, res, lat)) in enumerate(zip(reqs, got)):
+        t_s, r_s = single(core, q)
+        assert total == t_s, i
+        assert np.array_equal(res, r_s), i
+    assert got[0][0] > 10_000_000  # far more sites in range than the job's hit slice holds
