@@ -95,3 +95,26 @@ def test_batch_of_the_64_seed_workload(core):
     assert len(small) >= 30
     for i in small + large:
         check_against_reference(searches[i], *batch[i], f"64-seed batch request {i}")
+
+
+def test_batch_low_threshold_wide_requests(core):
+    """Low thresholds on areas 4+ periods wide run as grouped bands with exact counts (their own
+    launch class) inside the batch, beside bounded grouped and independent-band searches; every
+    result equals the single search's and the reference's."""
+    searches = [
+        Search(seed=51, center_x=-400_000, center_z=200_000, radius=300_000, min_size=44, max_results=3000),
+        Search(seed=-52, center_x=0, center_z=0, radius=280_000, min_size=43, max_size=50, rd_min=100_000,
+               max_results=1000),
+        Search(seed=53, center_x=1_000_000, center_z=-1_000_000, radius=150_000, min_size=52, max_results=200),
+        Search(seed=54, center_x=7, center_z=-7, radius=15_000, min_size=46, max_results=500),
+    ]
+    single = singles(core, searches)
+    assert core.lib.get_gpu_v1_algorithm() in (100, 300)  # the last, small search
+    core.lib.reset_cancel()
+    core.search(searches[0].seed, searches[0].radius, searches[0].min_size, 221, 0, searches[0].center_x,
+                searches[0].center_z, 10)
+    assert core.lib.get_gpu_v1_algorithm() == 230  # grouped bands, exact counts
+    batch = core.search_batch(searches)
+    check_same(batch, single)
+    for i, (q, (total, res)) in enumerate(zip(searches, batch)):
+        check_against_reference(q, total, res, f"low-threshold batch request {i}")
